@@ -1,0 +1,195 @@
+/*
+ * episdet.h -- C-ABI of the B200 epistasis-search library (libepisdet.so).
+ *
+ * Exhaustive 2-way / 3-way epistasis detection over binarized genotype bit
+ * planes, K2 or mutual-information scoring, best set by an FP64 re-score.
+ *
+ * Every entry point replaces one role of hiperbio/tensor-episdet:
+ *   episdet_search          <- EpistasisDetectionSearch(), src/search-pairs.cu:9
+ *                              and src/search-triplets.cu:8 (declared in
+ *                              include/search-pairs.hpp:4, search-triplets.hpp:4);
+ *                              the order (pairs/triplets) and score (K2/MI),
+ *                              fixed at build time there by -DTRIPLETS and
+ *                              -DMI_SCORE (Makefile:8-22), are options here.
+ *   episdet_search_batched  <- no counterpart (one dataset per process there,
+ *                              src/tensor-episdet.cu:159-172); many cohorts in
+ *                              one persistent launch.
+ *   episdet_search_perm     <- no counterpart (one label vector there); many
+ *                              phenotype permutations of one cohort.
+ *   episdet_read_dataset    <- the descriptor/.bin loader of
+ *                              src/tensor-episdet.cu:58-148.
+ *   episdet_n_choose_k      <- n_choose_k(), src/helper.cu:758-768.
+ *
+ * Data format (unchanged from the reference, src/tensor-episdet.cu:111-148,
+ * include/helper.hpp:10-25): one uint32 array per class laid out
+ * [SNP][genotype g in {0,1}][W] with W = ceil(n/1024)*32 words; sample s of a
+ * row sits in word s/32 at bit 31 - s%32.  Genotype 2 is implied (neither
+ * plane set).  Padding bits must be zero and the two planes of a row must be
+ * disjoint; inputs that break this are rejected with EPISDET_ERR_INVALID_INPUT
+ * (the reference silently produced undefined counts for them).
+ *
+ * Errors: every call returns an episdet_status; episdet_last_error() gives a
+ * thread-local message for the last failure.  No call exits or traps.
+ */
+#ifndef EPISDET_H_
+#define EPISDET_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EPISDET_ABI_VERSION 1
+
+typedef enum episdet_status {
+    EPISDET_OK = 0,
+    EPISDET_ERR_INVALID_ARGUMENT = 1, /* bad sizes, null pointers, unknown option */
+    EPISDET_ERR_INVALID_INPUT = 2,    /* padding bits set or genotype planes overlap */
+    EPISDET_ERR_NO_DEVICE = 3,        /* no usable sm_100 device */
+    EPISDET_ERR_CUDA = 4,             /* a CUDA runtime call failed */
+    EPISDET_ERR_OUT_OF_MEMORY = 5,
+    EPISDET_ERR_TIMEOUT = 6,          /* a bounded device wait gave up */
+    EPISDET_ERR_IO = 7,               /* descriptor or .bin file problem */
+    EPISDET_ERR_UNSUPPORTED = 8,
+    EPISDET_ERR_INTERNAL = 9
+} episdet_status;
+
+enum { EPISDET_SCORE_K2 = 0, EPISDET_SCORE_MI = 1 };
+enum { EPISDET_HOST = 0, EPISDET_DEVICE = 1 };
+
+/* Counting engine.  AUTO picks the tcgen05 tensor-core path. */
+enum { EPISDET_ENGINE_AUTO = 0, EPISDET_ENGINE_TENSOR = 1, EPISDET_ENGINE_SIMT = 2 };
+
+/* options.flags */
+#define EPISDET_FLAG_PROGRESS 0x1u     /* print the reference's "Outer loop iteration" lines */
+#define EPISDET_FLAG_NO_VALIDATE 0x2u  /* skip the padding / plane-overlap check */
+
+/* One cohort split into cases and controls (the reference's two .bin files). */
+typedef struct episdet_dataset {
+    const uint32_t* cases;    /* [num_snps][2][episdet_class_words(num_cases)] */
+    const uint32_t* controls; /* [num_snps][2][episdet_class_words(num_controls)] */
+    int32_t num_snps;         /* M >= order, M <= 2^21 - 1 */
+    int32_t num_cases;        /* >= 1 */
+    int32_t num_controls;     /* >= 1 */
+    int32_t memory;           /* EPISDET_HOST or EPISDET_DEVICE (current device) */
+} episdet_dataset;
+
+/* One cohort without a class split (all samples as one plane set). */
+typedef struct episdet_cohort {
+    const uint32_t* planes;   /* [num_snps][2][episdet_class_words(num_samples)] */
+    int32_t num_snps;
+    int32_t num_samples;
+    int32_t memory;
+} episdet_cohort;
+
+typedef struct episdet_options {
+    int32_t order;        /* 2 (pairs) or 3 (triplets) */
+    int32_t score;        /* EPISDET_SCORE_K2 (minimised) or EPISDET_SCORE_MI (maximised) */
+    int32_t top_k;        /* FP32 candidates re-scored in FP64; 1..4096, default 1024 */
+    int32_t device;       /* CUDA device ordinal, default 0 */
+    int32_t engine;       /* EPISDET_ENGINE_* */
+    int32_t first_begin;  /* evaluate only sets whose first SNP is in [first_begin, first_end) */
+    int32_t first_end;    /* 0 -> num_snps */
+    uint32_t flags;       /* EPISDET_FLAG_* */
+    int32_t reserved[8];
+} episdet_options;
+
+typedef struct episdet_result {
+    uint32_t snps[3];         /* best set (FP64 re-score, lowest index on ties); snps[2] = 0 for pairs */
+    uint64_t packed_indices;  /* reference packing: pairs a|b<<32 (src/helper.cu:690),
+                                 triplets x|y<<21|z<<42 (src/helper.cu:576) */
+    double score;             /* FP64 score of the best set */
+    float score_fp32;         /* FP32 epilogue score of the same set */
+    int32_t top_count;        /* entries written to top_* */
+    int64_t sets_evaluated;   /* C(M,k) restricted to the first_begin/end slab */
+    int64_t rounds;           /* reference block-round count (BLOCK_SIZE 256) */
+    double seconds;           /* wall time of the call (the reference's searchTime) */
+    double device_ms;         /* device time of the counting+scoring launches */
+    uint64_t kernel_launches; /* kernels this call launched */
+    /* Optional caller-owned outputs of capacity top_capacity (may be NULL). */
+    int32_t top_capacity;
+    uint32_t* top_snps;       /* [top_capacity][3] in FP32 rank order */
+    float* top_fp32;
+    double* top_fp64;
+} episdet_result;
+
+/* Words per genotype plane row for a class of n samples: ceil(n/1024)*32. */
+int32_t episdet_class_words(int32_t num_samples);
+
+void episdet_default_options(episdet_options* opts);
+
+/* Replaces EpistasisDetectionSearch (src/search-pairs.cu:9, src/search-triplets.cu:8). */
+episdet_status episdet_search(const episdet_dataset* data, const episdet_options* opts, episdet_result* result);
+
+/* Many independent cohorts (uneven SNP and sample counts) in one persistent
+ * launch over a shared tile queue.  opts[i] gives cohort i's order/score;
+ * results[i] receives its answer. */
+episdet_status episdet_search_batched(const episdet_dataset* cohorts, const episdet_options* opts, int32_t count,
+                                      episdet_result* results);
+
+/* Phenotype permutations of one cohort: labels is [num_labels][class_words(num_samples)],
+ * bit = 1 marks a case.  results[i] is the best pair/triplet under label i. */
+episdet_status episdet_search_perm(const episdet_cohort* cohort, const uint32_t* labels, int32_t num_labels,
+                                   const episdet_options* opts, episdet_result* results);
+
+/* Reads the reference's 5-line dataset descriptor and its two .bin files
+ * (src/tensor-episdet.cu:58-148) into malloc'd arrays; free with episdet_free_dataset. */
+episdet_status episdet_read_dataset(const char* descriptor_path, episdet_dataset* out);
+void episdet_free_dataset(episdet_dataset* data);
+
+/* Writes a dataset in the reference's format: descriptor + <stem>.cases.bin + <stem>.controls.bin. */
+episdet_status episdet_write_dataset(const char* descriptor_path, const episdet_dataset* data);
+
+/* Seeded synthetic data (Hardy-Weinberg genotypes, optional planted sets).
+ * planted: up to 2 sets of `order` SNP indices (flat array, -1 terminated or
+ * num_planted sets); penetrance: P(case) = base, or base + effect for each
+ * planted set whose SNPs all carry a minor allele. */
+typedef struct episdet_synth {
+    uint64_t seed;
+    int32_t num_snps;
+    int32_t num_cases;
+    int32_t num_controls;
+    float maf_min, maf_max;     /* minor-allele frequency ~ U[maf_min, maf_max] */
+    int32_t num_planted;        /* 0, 1 or 2 planted sets */
+    int32_t planted_order;      /* 2 or 3 */
+    int32_t planted[2][3];
+    float planted_maf;          /* > 0: fixed MAF for planted SNPs */
+    float base_risk;            /* P(case) baseline, e.g. 0.5 */
+    float effect;               /* added per planted set carried, e.g. 0.25 */
+} episdet_synth;
+
+/* Fills caller-allocated host arrays sized for the reference format. */
+episdet_status episdet_generate(const episdet_synth* spec, uint32_t* cases, uint32_t* controls);
+/* One plane set over num_samples individuals with independent labels. */
+episdet_status episdet_generate_cohort(uint64_t seed, int32_t num_snps, int32_t num_samples, float maf_min,
+                                       float maf_max, uint32_t* planes);
+/* num_labels label vectors; vector 0 has exactly num_cases cases (the first
+ * num_cases individuals), the others are seeded random permutations of it. */
+episdet_status episdet_generate_labels(uint64_t seed, int32_t num_samples, int32_t num_cases, int32_t num_labels,
+                                       uint32_t* labels);
+
+uint64_t episdet_n_choose_k(uint32_t n, uint32_t k);
+const char* episdet_status_string(episdet_status s);
+const char* episdet_last_error(void);
+int32_t episdet_abi_version(void);
+
+/* Frees the per-device workspace the library keeps between calls. */
+episdet_status episdet_release_workspace(int32_t device);
+
+#ifdef __cplusplus
+}
+#endif
+
+#ifdef __cplusplus
+/* Reference-compatible entry point (C++ linkage, cudaError_t return), one
+ * variant per link: libepisdet_compat_{pairs,triplets}_{k2,mi}.a defines
+ *   cudaError_t EpistasisDetectionSearch(unsigned int* cases, unsigned int* controls,
+ *       int numSNPs, int numCases, int numControls, uint numSNPsWithPadding,
+ *       int numCasesWithPadding, int numControlsWithPadding, int* roundsCounter,
+ *       double* searchTime, float* outputFromGpu, unsigned long long* packedIndices);
+ * with the semantics of src/search-pairs.cu:9 / src/search-triplets.cu:8. */
+#endif
+
+#endif /* EPISDET_H_ */

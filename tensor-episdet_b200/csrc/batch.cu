@@ -1,0 +1,148 @@
+// batch.cu -- many cohorts and many phenotype permutations per call.
+//
+// Neither has a counterpart in hiperbio/tensor-episdet, which searches one
+// dataset with one label vector per process (src/tensor-episdet.cu:159-172).
+// A permutation is applied on the GPU: a label vector splits the cohort's
+// sample columns into case and control plane sets in the reference layout,
+// which then go through the ordinary search with device-resident inputs.
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "episdet.h"
+#include "host_util.h"
+#include "search_internal.h"
+
+namespace episdet {
+
+// Gathers sample columns idx[0..n_out) of every plane row into a fresh
+// reference-layout row of W_out words (MSB-first, zero padding).
+__global__ void __launch_bounds__(256) gather_columns_kernel(const uint32_t* __restrict__ planes, int rows, int W_in,
+                                                             const int* __restrict__ idx, int n_out, int W_out,
+                                                             uint32_t* __restrict__ out) {
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)rows * W_out) return;
+    int r = (int)(t / W_out), ow = (int)(t % W_out);
+    const uint32_t* src = planes + (size_t)r * W_in;
+    uint32_t v = 0;
+    int base = ow * 32;
+#pragma unroll 4
+    for (int b = 0; b < 32; ++b) {
+        int s = base + b;
+        if (s < n_out) {
+            int j = __ldg(idx + s);
+            v |= ((__ldg(src + (j >> 5)) >> (31 - (j & 31))) & 1u) << (31 - b);
+        }
+    }
+    out[(size_t)r * W_out + ow] = v;
+}
+
+}  // namespace episdet
+
+using namespace episdet;
+
+// Prefixes the current error message (copied first: it is the output buffer too).
+static episdet_status with_prefix(episdet_status st, const char* what, int i) {
+    char msg[900];
+    snprintf(msg, sizeof(msg), "%s", episdet_last_error());
+    return set_error(st, "%s %d: %s", what, i, msg);
+}
+
+extern "C" episdet_status episdet_search_batched(const episdet_dataset* cohorts, const episdet_options* opts,
+                                                 int32_t count, episdet_result* results) {
+    clear_error();
+    if (!cohorts || !opts || !results || count < 1)
+        return set_error(EPISDET_ERR_INVALID_ARGUMENT, "batched search needs cohorts, options and results");
+    std::vector<episdet_options> os((size_t)count);
+    for (int32_t i = 0; i < count; ++i) {
+        episdet_status st = check_options(&opts[i], cohorts[i].num_snps, &os[i]);
+        if (st == EPISDET_OK) st = check_dataset(&cohorts[i], os[i].order);
+        if (st != EPISDET_OK) return with_prefix(st, "cohort", i);
+        if (os[i].device != os[0].device)
+            return set_error(EPISDET_ERR_INVALID_ARGUMENT, "all cohorts of a batch run on one device");
+    }
+    Workspace* w = nullptr;
+    episdet_status st = get_workspace(os[0].device, &w);
+    if (st != EPISDET_OK) return st;
+    std::lock_guard<std::mutex> lock(w->mu);
+    for (int32_t i = 0; i < count; ++i) {
+        st = search_locked(w, &cohorts[i], os[i], &results[i]);
+        if (st != EPISDET_OK) return with_prefix(st, "cohort", i);
+    }
+    return EPISDET_OK;
+}
+
+extern "C" episdet_status episdet_search_perm(const episdet_cohort* cohort, const uint32_t* labels,
+                                              int32_t num_labels, const episdet_options* opts,
+                                              episdet_result* results) {
+    clear_error();
+    if (!cohort || !cohort->planes || !labels || num_labels < 1 || !results)
+        return set_error(EPISDET_ERR_INVALID_ARGUMENT, "permutation search needs a cohort, labels and results");
+    if (cohort->memory != EPISDET_HOST && cohort->memory != EPISDET_DEVICE)
+        return set_error(EPISDET_ERR_INVALID_ARGUMENT, "unknown memory kind");
+    const int M = cohort->num_snps, n = cohort->num_samples;
+    if (M < 2 || n < 2 || M > (1 << 21) - 1) return set_error(EPISDET_ERR_INVALID_ARGUMENT, "bad cohort sizes");
+    episdet_options o;
+    episdet_status st = check_options(opts, M, &o);
+    if (st != EPISDET_OK) return st;
+    Workspace* w = nullptr;
+    st = get_workspace(o.device, &w);
+    if (st != EPISDET_OK) return st;
+    std::lock_guard<std::mutex> lock(w->mu);
+    CUDA_TRY(cudaSetDevice(o.device));
+    const int W = episdet_class_words(n);
+    const size_t plane_words = (size_t)M * 2 * W;
+    const uint32_t* d_planes = cohort->planes;
+    if (cohort->memory == EPISDET_HOST) {
+        CUDA_TRY(w->perm_planes.ensure(sizeof(uint32_t) * plane_words));
+        CUDA_TRY(cudaMemcpyAsync(w->perm_planes.p, cohort->planes, sizeof(uint32_t) * plane_words,
+                                 cudaMemcpyHostToDevice, w->st));
+        d_planes = (const uint32_t*)w->perm_planes.p;
+    }
+    std::vector<uint32_t> lab((size_t)W);
+    std::vector<int> idx((size_t)n);
+    for (int32_t p = 0; p < num_labels; ++p) {
+        if (cohort->memory == EPISDET_HOST)
+            memcpy(lab.data(), labels + (size_t)p * W, sizeof(uint32_t) * W);
+        else {
+            CUDA_TRY(cudaMemcpyAsync(lab.data(), labels + (size_t)p * W, sizeof(uint32_t) * W, cudaMemcpyDeviceToHost,
+                                     w->st));
+            CUDA_TRY(cudaStreamSynchronize(w->st));
+        }
+        int nc = 0;
+        for (int s = 0; s < n; ++s)
+            if ((lab[s / 32] >> (31 - s % 32)) & 1u) idx[nc++] = s;
+        int nn = nc;
+        for (int s = 0; s < n; ++s)
+            if (!((lab[s / 32] >> (31 - s % 32)) & 1u)) idx[nn++] = s;
+        nn -= nc;
+        if (nc < 1 || nn < 1) return set_error(EPISDET_ERR_INVALID_ARGUMENT, "label %d leaves a class empty", p);
+        const int Wc = episdet_class_words(nc), Wn = episdet_class_words(nn);
+        CUDA_TRY(w->perm_idx.ensure(sizeof(int) * (size_t)n));
+        CUDA_TRY(w->perm_cls[0].ensure(sizeof(uint32_t) * (size_t)M * 2 * Wc));
+        CUDA_TRY(w->perm_cls[1].ensure(sizeof(uint32_t) * (size_t)M * 2 * Wn));
+        CUDA_TRY(cudaMemcpyAsync(w->perm_idx.p, idx.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, w->st));
+        long t0 = (long)2 * M * Wc, t1 = (long)2 * M * Wn;
+        gather_columns_kernel<<<(unsigned)((t0 + 255) / 256), 256, 0, w->st>>>(d_planes, 2 * M, W,
+                                                                                (const int*)w->perm_idx.p, nc, Wc,
+                                                                                (uint32_t*)w->perm_cls[0].p);
+        CUDA_TRY(cudaGetLastError());
+        gather_columns_kernel<<<(unsigned)((t1 + 255) / 256), 256, 0, w->st>>>(d_planes, 2 * M, W,
+                                                                                (const int*)w->perm_idx.p + nc, nn, Wn,
+                                                                                (uint32_t*)w->perm_cls[1].p);
+        CUDA_TRY(cudaGetLastError());
+        episdet_dataset d;
+        d.cases = (const uint32_t*)w->perm_cls[0].p;
+        d.controls = (const uint32_t*)w->perm_cls[1].p;
+        d.num_snps = M;
+        d.num_cases = nc;
+        d.num_controls = nn;
+        d.memory = EPISDET_DEVICE;
+        st = check_dataset(&d, o.order);
+        if (st == EPISDET_OK) st = search_locked(w, &d, o, &results[p]);
+        if (st != EPISDET_OK) return with_prefix(st, "label", p);
+        results[p].kernel_launches += 2;
+    }
+    return EPISDET_OK;
+}

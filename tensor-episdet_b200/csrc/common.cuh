@@ -1,0 +1,247 @@
+// common.cuh -- device helpers shared by every counting engine: candidate
+// keys, the per-CTA top-K buffer, genotype-table derivation and K2/MI scoring.
+//
+// Scoring follows include/scoring.hpp of hiperbio/tensor-episdet: CALC_K2
+// (scoring.hpp:5-7) and CALC_MI (scoring.hpp:9-16) visited cell by cell in
+// index order (scoring.hpp:41-45, :78-84).  Every FP operation is an explicit
+// round-to-nearest intrinsic so that the result is reproducible bit for bit
+// by a CPU running the same sequence (no contraction, no reassociation).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace episdet {
+
+constexpr int kMaxTopK = 2048;
+
+// Candidate: 32-bit orderable FP32 score key (smaller = better for both K2
+// and MI) and the lexicographic set key (pairs a<<32|b, triplets
+// x<<42|y<<21|z).  Order: key, then set.
+struct __align__(16) Cand {
+    uint32_t key;
+    uint32_t pad;
+    uint64_t set;
+};
+
+__host__ __device__ inline bool cand_better(const Cand& a, const Cand& b) {
+    return a.key < b.key || (a.key == b.key && a.set < b.set);
+}
+
+__host__ __device__ inline Cand cand_worst() {
+    Cand c;
+    c.key = 0xFFFFFFFFu;
+    c.pad = 0;
+    c.set = ~0ull;
+    return c;
+}
+
+__device__ inline uint32_t score_key(float s, bool maximize) {
+    if (maximize) s = -s;
+    uint32_t u = __float_as_uint(s);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+__host__ __device__ inline float key_score(uint32_t key, bool maximize) {
+    uint32_t u = (key & 0x80000000u) ? (key & 0x7FFFFFFFu) : ~key;
+    float s;
+#ifdef __CUDA_ARCH__
+    s = __uint_as_float(u);
+#else
+    __builtin_memcpy(&s, &u, 4);
+#endif
+    return maximize ? -s : s;
+}
+
+__host__ __device__ inline uint64_t set_key3(uint32_t x, uint32_t y, uint32_t z) {
+    return ((uint64_t)x << 42) | ((uint64_t)y << 21) | (uint64_t)z;
+}
+__host__ __device__ inline uint64_t set_key2(uint32_t a, uint32_t b) { return ((uint64_t)a << 32) | (uint64_t)b; }
+
+// ------------------------------------------------------------------ scoring
+struct ScoreTables {
+    const float* t32;   // K2: lnGamma(v+1); MI: log2(v/N), index 0 -> 0
+    const double* t64;
+    float inv_n32;
+    float hy32;
+    double inv_n64;
+    double hy64;
+    int score;          // 0 = K2, 1 = MI
+};
+
+// One K2 cell term, scoring.hpp:5-7: t[ctrl] + t[case] - t[ctrl+case+1].
+__device__ __forceinline__ float k2_term32(const float* __restrict__ t, int cs, int cn) {
+    return __fsub_rn(__fadd_rn(__ldg(t + cn), __ldg(t + cs)), __ldg(t + cn + cs + 1));
+}
+
+template <int NC>
+__device__ __forceinline__ float score32(const ScoreTables& T, const int* cs, const int* cn) {
+    if (T.score == 0) {
+        float s = 0.0f;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) s = __fadd_rn(s, k2_term32(T.t32, cs[c], cn[c]));
+        return fabsf(s);
+    }
+    float ha = 0.0f, hx = 0.0f;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        float pc = __fmul_rn(__int2float_rn(cs[c]), T.inv_n32);
+        ha = __fmaf_rn(-pc, __ldg(T.t32 + cs[c]), ha);
+        float pn = __fmul_rn(__int2float_rn(cn[c]), T.inv_n32);
+        ha = __fmaf_rn(-pn, __ldg(T.t32 + cn[c]), ha);
+        hx = __fmaf_rn(-__fadd_rn(pc, pn), __ldg(T.t32 + cs[c] + cn[c]), hx);
+    }
+    return __fsub_rn(__fadd_rn(hx, T.hy32), ha);
+}
+
+template <int NC>
+__device__ __forceinline__ double score64(const ScoreTables& T, const int* cs, const int* cn) {
+    if (T.score == 0) {
+        double s = 0.0;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            double term = __dsub_rn(__dadd_rn(T.t64[cn[c]], T.t64[cs[c]]), T.t64[cn[c] + cs[c] + 1]);
+            s = __dadd_rn(s, term);
+        }
+        return fabs(s);
+    }
+    double ha = 0.0, hx = 0.0;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        double pc = __dmul_rn((double)cs[c], T.inv_n64);
+        ha = __fma_rn(-pc, T.t64[cs[c]], ha);
+        double pn = __dmul_rn((double)cn[c], T.inv_n64);
+        ha = __fma_rn(-pn, T.t64[cn[c]], ha);
+        hx = __fma_rn(-__dadd_rn(pc, pn), T.t64[cs[c] + cn[c]], hx);
+    }
+    return __dsub_rn(__dadd_rn(hx, T.hy64), ha);
+}
+
+// --------------------------------------------------------------- derivation
+// 2-way table, src/helper.cu:634-662: t[i*3+j] for i,j<2 hold the AND cells;
+// pa/pb are the genotype counts (g2 = n - g0 - g1) of the two SNPs.
+__device__ __forceinline__ void derive9(int t[9], const int pa[3], const int pb[3]) {
+    t[0 * 3 + 2] = pa[0] - (t[0 * 3 + 0] + t[0 * 3 + 1]);
+    t[1 * 3 + 2] = pa[1] - (t[1 * 3 + 0] + t[1 * 3 + 1]);
+    t[2 * 3 + 0] = pb[0] - (t[0 * 3 + 0] + t[1 * 3 + 0]);
+    t[2 * 3 + 1] = pb[1] - (t[0 * 3 + 1] + t[1 * 3 + 1]);
+    t[2 * 3 + 2] = pa[2] - (t[2 * 3 + 0] + t[2 * 3 + 1]);
+}
+
+#define EPI_C3(i, j, k) ((i) * 9 + (j) * 3 + (k))
+// 3-way table, src/helper.cu:494-548 with the macros of include/helper.hpp:34-51.
+// On entry t holds the 8 AND cells (i,j,k < 2); xy/xz/yz are 9-cell pair tables.
+__device__ __forceinline__ void derive27(int t[27], const int xy[9], const int xz[9], const int yz[9]) {
+    t[EPI_C3(0, 0, 2)] = xy[0] - (t[EPI_C3(0, 0, 0)] + t[EPI_C3(0, 0, 1)]);
+    t[EPI_C3(0, 1, 2)] = xy[1] - (t[EPI_C3(0, 1, 0)] + t[EPI_C3(0, 1, 1)]);
+    t[EPI_C3(0, 2, 0)] = xz[0] - (t[EPI_C3(0, 0, 0)] + t[EPI_C3(0, 1, 0)]);
+    t[EPI_C3(0, 2, 1)] = xz[1] - (t[EPI_C3(0, 0, 1)] + t[EPI_C3(0, 1, 1)]);
+    t[EPI_C3(0, 2, 2)] = xz[2] - (t[EPI_C3(0, 0, 2)] + t[EPI_C3(0, 1, 2)]);
+    t[EPI_C3(1, 0, 2)] = xy[3] - (t[EPI_C3(1, 0, 0)] + t[EPI_C3(1, 0, 1)]);
+    t[EPI_C3(1, 1, 2)] = xy[4] - (t[EPI_C3(1, 1, 0)] + t[EPI_C3(1, 1, 1)]);
+    t[EPI_C3(1, 2, 0)] = xz[3] - (t[EPI_C3(1, 0, 0)] + t[EPI_C3(1, 1, 0)]);
+    t[EPI_C3(1, 2, 1)] = xz[4] - (t[EPI_C3(1, 0, 1)] + t[EPI_C3(1, 1, 1)]);
+    t[EPI_C3(1, 2, 2)] = xz[5] - (t[EPI_C3(1, 0, 2)] + t[EPI_C3(1, 1, 2)]);
+    t[EPI_C3(2, 0, 0)] = yz[0] - (t[EPI_C3(0, 0, 0)] + t[EPI_C3(1, 0, 0)]);
+    t[EPI_C3(2, 0, 1)] = yz[1] - (t[EPI_C3(0, 0, 1)] + t[EPI_C3(1, 0, 1)]);
+    t[EPI_C3(2, 0, 2)] = xy[6] - (t[EPI_C3(2, 0, 0)] + t[EPI_C3(2, 0, 1)]);
+    t[EPI_C3(2, 1, 0)] = yz[3] - (t[EPI_C3(0, 1, 0)] + t[EPI_C3(1, 1, 0)]);
+    t[EPI_C3(2, 1, 1)] = yz[4] - (t[EPI_C3(0, 1, 1)] + t[EPI_C3(1, 1, 1)]);
+    t[EPI_C3(2, 1, 2)] = xy[7] - (t[EPI_C3(2, 1, 0)] + t[EPI_C3(2, 1, 1)]);
+    t[EPI_C3(2, 2, 0)] = xz[6] - (t[EPI_C3(2, 0, 0)] + t[EPI_C3(2, 1, 0)]);
+    t[EPI_C3(2, 2, 1)] = xz[7] - (t[EPI_C3(2, 0, 1)] + t[EPI_C3(2, 1, 1)]);
+    t[EPI_C3(2, 2, 2)] = xz[8] - (t[EPI_C3(2, 0, 2)] + t[EPI_C3(2, 1, 2)]);
+}
+
+// 9-cell pair table from its 4 AND cells and the two SNPs' genotype counts
+// (the 2-way derivation of helper.cu:645-662; equal to the masked direct
+// count of helper.cu:58-194 for valid inputs).
+__device__ __forceinline__ void pair9_from4(int out[9], const uint4& and4, const int ma[3], const int mb[3]) {
+    out[0] = (int)and4.x;
+    out[1] = (int)and4.y;
+    out[3] = (int)and4.z;
+    out[4] = (int)and4.w;
+    derive9(out, ma, mb);
+}
+
+// ------------------------------------------------------- per-CTA top-K list
+// Shared-memory candidate buffer of capacity CAP (power of two).  Threads
+// offer() candidates better than the local threshold with a shared atomic;
+// callers compact() (all NT threads, between barriers) before the buffer can
+// overflow.  After compact() the first min(count, K) entries are sorted best
+// first and the threshold is the K-th entry.
+template <int CAP, int NT>
+struct LocalTopK {
+    Cand* buf;     // [CAP]
+    int* count;    // shared scalar
+    Cand* thr;     // shared scalar
+    int k;
+    int tid;
+
+    __device__ void offer(const Cand& c, const Cand& thr_reg) const {
+        if (cand_better(c, thr_reg)) {
+            int slot = atomicAdd(count, 1);
+            buf[slot] = c;
+        }
+    }
+
+    // Bitonic sort of buf[0..CAP) with entries >= n set to worst; requires a
+    // barrier functor covering exactly the NT participating threads.
+    template <class Bar>
+    __device__ void compact(Bar bar) const {
+        int n = *count;
+        for (int i = n + tid; i < CAP; i += NT) buf[i] = cand_worst();
+        bar();
+        for (int kk = 2; kk <= CAP; kk <<= 1) {
+            for (int j = kk >> 1; j > 0; j >>= 1) {
+                for (int i = tid; i < CAP; i += NT) {
+                    int ixj = i ^ j;
+                    if (ixj > i) {
+                        Cand a = buf[i], b = buf[ixj];
+                        bool up = (i & kk) == 0;
+                        if (up ? cand_better(b, a) : cand_better(a, b)) {
+                            buf[i] = b;
+                            buf[ixj] = a;
+                        }
+                    }
+                }
+                bar();
+            }
+        }
+        if (tid == 0) {
+            int m = n < k ? n : k;
+            *count = m;
+            *thr = (m >= k) ? buf[k - 1] : cand_worst();
+        }
+        bar();
+    }
+
+    template <class Bar>
+    __device__ void load(const Cand* __restrict__ slot, int slot_count, Bar bar) const {
+        for (int i = tid; i < slot_count; i += NT) buf[i] = slot[i];
+        if (tid == 0) {
+            *count = slot_count;
+            *thr = (slot_count >= k) ? slot[k - 1] : cand_worst();
+        }
+        bar();
+    }
+
+    template <class Bar>
+    __device__ void store(Cand* __restrict__ slot, int* __restrict__ slot_count, Bar bar) const {
+        compact(bar);
+        int n = *count;
+        for (int i = tid; i < n; i += NT) slot[i] = buf[i];
+        if (tid == 0) *slot_count = n;
+    }
+};
+
+struct BarAll {
+    __device__ void operator()() const { __syncthreads(); }
+};
+
+// Named barrier over `n` threads (multiple of 32) of one CTA.
+struct BarNamed {
+    int id, n;
+    __device__ void operator()() const { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
+};
+
+}  // namespace episdet

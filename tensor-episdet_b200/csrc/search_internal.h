@@ -1,0 +1,71 @@
+// search_internal.h -- host-side workspace and helpers shared by the engines.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <mutex>
+
+#include "common.cuh"
+#include "device_data.cuh"
+#include "episdet.h"
+
+namespace episdet {
+
+episdet_status cuda_fail(cudaError_t e, const char* what);
+
+#define CUDA_TRY(x)                                     \
+    do {                                                \
+        cudaError_t e_ = (x);                           \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #x); \
+    } while (0)
+
+// Grow-only device allocation kept between calls.
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes);
+    void release();
+};
+
+struct Workspace {
+    int device = 0;
+    int sms = 0;
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    std::mutex mu;
+    DevBuf bits[2], marg[2], pair4[2], t32, t64, slots, counts, tiles, merged, mcount, fp64, flag;
+    DevBuf planes8;       // unpacked 0/1 byte operand rows (tensor engine)
+    DevBuf xsub[2];       // per-X sample-compacted operand rows (tensor engine, double buffered)
+    DevBuf xinfo;         // per-X segment tables (tensor engine)
+    DevBuf tensor_flag;   // device error / progress words of the tensor engine
+    DevBuf perm_planes, perm_cls[2], perm_idx;  // phenotype-permutation staging
+    int tab_score = -1, tab_nc = -1, tab_nn = -1;
+    float inv32 = 0.0f, hy32 = 0.0f;
+    double inv64 = 0.0, hy64 = 0.0;
+
+    void release_all() {
+        DevBuf* all[] = {&bits[0], &bits[1], &marg[0], &marg[1], &pair4[0], &pair4[1], &t32, &t64, &slots,
+                         &counts, &tiles, &merged, &mcount, &fp64, &flag, &planes8, &xsub[0], &xsub[1], &xinfo,
+                         &tensor_flag, &perm_planes, &perm_cls[0], &perm_cls[1], &perm_idx};
+        for (DevBuf* b : all) b->release();
+        tab_score = tab_nc = tab_nn = -1;
+    }
+};
+
+episdet_status get_workspace(int device, Workspace** out);
+episdet_status build_tables(Workspace* w, int score, int nc, int nn, ScoreTables* T);
+episdet_status stage_dataset(Workspace* w, const episdet_dataset* d, bool validate, DevData* D, uint64_t* launches);
+episdet_status prepare_slots(Workspace* w, int nslots, int k, Slots* S);
+episdet_status check_options(const episdet_options* in, int M, episdet_options* o);
+episdet_status check_dataset(const episdet_dataset* d, int order);
+
+// One search; the caller holds w->mu and has validated the options.
+episdet_status search_locked(Workspace* w, const episdet_dataset* data, const episdet_options& o,
+                             episdet_result* result);
+
+// Tensor-core engine (tensor.cu).  Fills S with the per-CTA candidate lists.
+episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const episdet_options& o, int fb, int fe,
+                          Slots* S, uint64_t* launches, bool progress);
+
+}  // namespace episdet

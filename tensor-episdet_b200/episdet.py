@@ -1,0 +1,337 @@
+"""Python binding of libepisdet.so (the B200 epistasis-search C-ABI).
+
+Mirrors the reference's search entry point, ``EpistasisDetectionSearch``
+(hiperbio/tensor-episdet src/search-pairs.cu:9, src/search-triplets.cu:8),
+with the same argument meanings, plus keyword-style helpers used by the tests
+and the benchmark.  Every call goes through the C-ABI declared in
+include/episdet.h; there is no Python or CPU fallback -- if the shared library
+is missing or was not built for this GPU, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libepisdet.so")
+
+SCORE_K2, SCORE_MI = 0, 1
+HOST, DEVICE = 0, 1
+ENGINE_AUTO, ENGINE_TENSOR, ENGINE_SIMT = 0, 1, 2
+FLAG_PROGRESS, FLAG_NO_VALIDATE = 0x1, 0x2
+
+STATUS = {
+    0: "EPISDET_OK",
+    1: "EPISDET_ERR_INVALID_ARGUMENT",
+    2: "EPISDET_ERR_INVALID_INPUT",
+    3: "EPISDET_ERR_NO_DEVICE",
+    4: "EPISDET_ERR_CUDA",
+    5: "EPISDET_ERR_OUT_OF_MEMORY",
+    6: "EPISDET_ERR_TIMEOUT",
+    7: "EPISDET_ERR_IO",
+    8: "EPISDET_ERR_UNSUPPORTED",
+    9: "EPISDET_ERR_INTERNAL",
+}
+
+# Every symbol include/episdet.h declares with C linkage.
+EXPORTED = [
+    "episdet_class_words", "episdet_default_options", "episdet_search", "episdet_search_batched",
+    "episdet_search_perm", "episdet_read_dataset", "episdet_free_dataset", "episdet_write_dataset",
+    "episdet_generate", "episdet_generate_cohort", "episdet_generate_labels", "episdet_n_choose_k",
+    "episdet_status_string", "episdet_last_error", "episdet_abi_version", "episdet_release_workspace",
+]
+
+
+class EpisdetError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+        self.name = STATUS.get(status, str(status))
+
+
+class Dataset(ctypes.Structure):
+    _fields_ = [("cases", ctypes.c_void_p), ("controls", ctypes.c_void_p), ("num_snps", ctypes.c_int32),
+                ("num_cases", ctypes.c_int32), ("num_controls", ctypes.c_int32), ("memory", ctypes.c_int32)]
+
+
+class Cohort(ctypes.Structure):
+    _fields_ = [("planes", ctypes.c_void_p), ("num_snps", ctypes.c_int32), ("num_samples", ctypes.c_int32),
+                ("memory", ctypes.c_int32)]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("order", ctypes.c_int32), ("score", ctypes.c_int32), ("top_k", ctypes.c_int32),
+                ("device", ctypes.c_int32), ("engine", ctypes.c_int32), ("first_begin", ctypes.c_int32),
+                ("first_end", ctypes.c_int32), ("flags", ctypes.c_uint32), ("reserved", ctypes.c_int32 * 8)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("snps", ctypes.c_uint32 * 3), ("packed_indices", ctypes.c_uint64), ("score", ctypes.c_double),
+                ("score_fp32", ctypes.c_float), ("top_count", ctypes.c_int32), ("sets_evaluated", ctypes.c_int64),
+                ("rounds", ctypes.c_int64), ("seconds", ctypes.c_double), ("device_ms", ctypes.c_double),
+                ("kernel_launches", ctypes.c_uint64), ("top_capacity", ctypes.c_int32),
+                ("top_snps", ctypes.POINTER(ctypes.c_uint32)), ("top_fp32", ctypes.POINTER(ctypes.c_float)),
+                ("top_fp64", ctypes.POINTER(ctypes.c_double))]
+
+
+class Synth(ctypes.Structure):
+    _fields_ = [("seed", ctypes.c_uint64), ("num_snps", ctypes.c_int32), ("num_cases", ctypes.c_int32),
+                ("num_controls", ctypes.c_int32), ("maf_min", ctypes.c_float), ("maf_max", ctypes.c_float),
+                ("num_planted", ctypes.c_int32), ("planted_order", ctypes.c_int32),
+                ("planted", (ctypes.c_int32 * 3) * 2), ("planted_maf", ctypes.c_float),
+                ("base_risk", ctypes.c_float), ("effect", ctypes.c_float)]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Loads libepisdet.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FileNotFoundError(f"{LIB_PATH} is missing: build it with `make -C {HERE}`")
+    L = ctypes.CDLL(LIB_PATH)
+    P = ctypes.POINTER
+    L.episdet_class_words.argtypes = [ctypes.c_int32]
+    L.episdet_class_words.restype = ctypes.c_int32
+    L.episdet_default_options.argtypes = [P(Options)]
+    L.episdet_search.argtypes = [P(Dataset), P(Options), P(Result)]
+    L.episdet_search.restype = ctypes.c_int
+    L.episdet_search_batched.argtypes = [P(Dataset), P(Options), ctypes.c_int32, P(Result)]
+    L.episdet_search_batched.restype = ctypes.c_int
+    L.episdet_search_perm.argtypes = [P(Cohort), ctypes.c_void_p, ctypes.c_int32, P(Options), P(Result)]
+    L.episdet_search_perm.restype = ctypes.c_int
+    L.episdet_read_dataset.argtypes = [ctypes.c_char_p, P(Dataset)]
+    L.episdet_read_dataset.restype = ctypes.c_int
+    L.episdet_free_dataset.argtypes = [P(Dataset)]
+    L.episdet_write_dataset.argtypes = [ctypes.c_char_p, P(Dataset)]
+    L.episdet_write_dataset.restype = ctypes.c_int
+    L.episdet_generate.argtypes = [P(Synth), ctypes.c_void_p, ctypes.c_void_p]
+    L.episdet_generate.restype = ctypes.c_int
+    L.episdet_generate_cohort.argtypes = [ctypes.c_uint64, ctypes.c_int32, ctypes.c_int32, ctypes.c_float,
+                                          ctypes.c_float, ctypes.c_void_p]
+    L.episdet_generate_cohort.restype = ctypes.c_int
+    L.episdet_generate_labels.argtypes = [ctypes.c_uint64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                          ctypes.c_void_p]
+    L.episdet_generate_labels.restype = ctypes.c_int
+    L.episdet_n_choose_k.argtypes = [ctypes.c_uint32, ctypes.c_uint32]
+    L.episdet_n_choose_k.restype = ctypes.c_uint64
+    L.episdet_status_string.argtypes = [ctypes.c_int]
+    L.episdet_status_string.restype = ctypes.c_char_p
+    L.episdet_last_error.restype = ctypes.c_char_p
+    L.episdet_abi_version.restype = ctypes.c_int32
+    L.episdet_release_workspace.argtypes = [ctypes.c_int32]
+    L.episdet_release_workspace.restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def _check(status: int) -> None:
+    if status != 0:
+        raise EpisdetError(status, lib().episdet_last_error().decode(errors="replace"))
+
+
+def class_words(n: int) -> int:
+    return ((n + 1023) // 1024) * 32
+
+
+def n_choose_k(n: int, k: int) -> int:
+    return int(lib().episdet_n_choose_k(n, k))
+
+
+# ------------------------------------------------------------------ data
+def empty_planes(num_snps: int, num_samples: int) -> np.ndarray:
+    return np.zeros((num_snps, 2, class_words(num_samples)), dtype=np.uint32)
+
+
+def generate(seed: int, num_snps: int, num_cases: int, num_controls: int, maf=(0.05, 0.5), planted=(),
+             planted_maf: float = 0.0, base_risk: float = 0.5, effect: float = 0.25):
+    """Seeded Hardy-Weinberg dataset in the reference's per-class plane format.
+
+    planted: up to two tuples of 2 or 3 SNP indices carrying the penetrance
+    effect.  Returns (cases, controls) uint32 arrays [M][2][W].
+    """
+    s = Synth()
+    s.seed, s.num_snps, s.num_cases, s.num_controls = seed, num_snps, num_cases, num_controls
+    s.maf_min, s.maf_max = maf
+    s.num_planted = len(planted)
+    s.planted_order = len(planted[0]) if planted else 3
+    for q, ps in enumerate(planted):
+        for e, v in enumerate(ps):
+            s.planted[q][e] = v
+    s.planted_maf, s.base_risk, s.effect = planted_maf, base_risk, effect
+    cases = empty_planes(num_snps, num_cases)
+    controls = empty_planes(num_snps, num_controls)
+    _check(lib().episdet_generate(ctypes.byref(s), cases.ctypes.data, controls.ctypes.data))
+    return cases, controls
+
+
+def generate_cohort(seed: int, num_snps: int, num_samples: int, maf=(0.05, 0.5)) -> np.ndarray:
+    planes = empty_planes(num_snps, num_samples)
+    _check(lib().episdet_generate_cohort(seed, num_snps, num_samples, maf[0], maf[1], planes.ctypes.data))
+    return planes
+
+
+def generate_labels(seed: int, num_samples: int, num_cases: int, num_labels: int) -> np.ndarray:
+    labels = np.zeros((num_labels, class_words(num_samples)), dtype=np.uint32)
+    _check(lib().episdet_generate_labels(seed, num_samples, num_cases, num_labels, labels.ctypes.data))
+    return labels
+
+
+def read_dataset(path: str):
+    d = Dataset()
+    _check(lib().episdet_read_dataset(path.encode(), ctypes.byref(d)))
+    try:
+        M, nc, nn = d.num_snps, d.num_cases, d.num_controls
+        wc, wn = class_words(nc), class_words(nn)
+        cases = np.ctypeslib.as_array(ctypes.cast(d.cases, ctypes.POINTER(ctypes.c_uint32)),
+                                      shape=(M * 2 * wc,)).copy().reshape(M, 2, wc)
+        controls = np.ctypeslib.as_array(ctypes.cast(d.controls, ctypes.POINTER(ctypes.c_uint32)),
+                                         shape=(M * 2 * wn,)).copy().reshape(M, 2, wn)
+    finally:
+        lib().episdet_free_dataset(ctypes.byref(d))
+    return cases, controls, nc, nn
+
+
+def write_dataset(path: str, cases: np.ndarray, controls: np.ndarray, num_cases: int, num_controls: int) -> None:
+    cases = np.ascontiguousarray(cases, dtype=np.uint32)
+    controls = np.ascontiguousarray(controls, dtype=np.uint32)
+    d = Dataset(cases.ctypes.data, controls.ctypes.data, cases.shape[0], num_cases, num_controls, HOST)
+    _check(lib().episdet_write_dataset(path.encode(), ctypes.byref(d)))
+
+
+# ---------------------------------------------------------------- search
+@dataclass
+class SearchResult:
+    snps: tuple
+    score: float
+    score_fp32: float
+    packed_indices: int
+    sets_evaluated: int
+    rounds: int
+    seconds: float
+    device_ms: float
+    kernel_launches: int
+    top_snps: np.ndarray = field(repr=False)
+    top_fp32: np.ndarray = field(repr=False)
+    top_fp64: np.ndarray = field(repr=False)
+
+
+def _ptr(a):
+    """(pointer, memory kind) of a numpy array or a CUDA tensor."""
+    if hasattr(a, "data_ptr") and getattr(a, "is_cuda", False):
+        return a.data_ptr(), DEVICE
+    if not (isinstance(a, np.ndarray) and a.dtype == np.uint32 and a.flags["C_CONTIGUOUS"]):
+        raise TypeError("planes must be C-contiguous uint32 numpy arrays or CUDA tensors")
+    return a.ctypes.data, HOST
+
+
+def make_options(order=3, score="k2", top_k=1024, device=0, engine="auto", first_begin=0, first_end=0,
+                 flags=0) -> Options:
+    o = Options()
+    lib().episdet_default_options(ctypes.byref(o))
+    o.order = order
+    o.score = {"k2": SCORE_K2, "mi": SCORE_MI}[score] if isinstance(score, str) else int(score)
+    o.top_k = top_k
+    o.device = device
+    o.engine = {"auto": ENGINE_AUTO, "tensor": ENGINE_TENSOR, "simt": ENGINE_SIMT}[engine] \
+        if isinstance(engine, str) else int(engine)
+    o.first_begin, o.first_end, o.flags = first_begin, first_end, flags
+    return o
+
+
+def _result_buffers(cap: int) -> Result:
+    r = Result()
+    r.top_capacity = cap
+    bufs = (np.zeros((cap, 3), dtype=np.uint32), np.zeros(cap, dtype=np.float32), np.zeros(cap, dtype=np.float64))
+    r.top_snps = bufs[0].ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+    r.top_fp32 = bufs[1].ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    r.top_fp64 = bufs[2].ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    return r, bufs
+
+
+def _to_result(order: int, r: Result, bufs) -> SearchResult:
+    n = r.top_count
+    return SearchResult(snps=tuple(int(v) for v in r.snps[:order]), score=r.score, score_fp32=r.score_fp32,
+                        packed_indices=int(r.packed_indices), sets_evaluated=int(r.sets_evaluated),
+                        rounds=int(r.rounds), seconds=r.seconds, device_ms=r.device_ms,
+                        kernel_launches=int(r.kernel_launches), top_snps=bufs[0][:n, :order].copy(),
+                        top_fp32=bufs[1][:n].copy(), top_fp64=bufs[2][:n].copy())
+
+
+def search(cases, controls, num_cases: int, num_controls: int, *, num_snps: Optional[int] = None, order: int = 3,
+           score="k2", top_k: int = 1024, device: int = 0, engine="auto", first_begin: int = 0, first_end: int = 0,
+           flags: int = 0) -> SearchResult:
+    """Exhaustive search; cases/controls are host uint32 arrays or CUDA tensors in the plane format."""
+    pc, mc = _ptr(cases)
+    pn, mn = _ptr(controls)
+    if mc != mn:
+        raise TypeError("cases and controls must live in the same memory")
+    M = num_snps if num_snps is not None else int(cases.shape[0])
+    d = Dataset(pc, pn, M, num_cases, num_controls, mc)
+    o = make_options(order, score, top_k, device, engine, first_begin, first_end, flags)
+    r, bufs = _result_buffers(top_k)
+    _check(lib().episdet_search(ctypes.byref(d), ctypes.byref(o), ctypes.byref(r)))
+    return _to_result(order, r, bufs)
+
+
+def search_batched(cohorts, options) -> list:
+    """cohorts: list of (cases, controls, num_cases, num_controls); options: list of dicts for make_options."""
+    n = len(cohorts)
+    ds = (Dataset * n)()
+    os_ = (Options * n)()
+    rs = (Result * n)()
+    keep = []
+    for i, ((c, k, nc, nn), opt) in enumerate(zip(cohorts, options)):
+        pc, mc = _ptr(c)
+        pn, _ = _ptr(k)
+        ds[i] = Dataset(pc, pn, int(c.shape[0]), nc, nn, mc)
+        os_[i] = make_options(**opt)
+        r, bufs = _result_buffers(os_[i].top_k)
+        rs[i] = r
+        keep.append(bufs)
+    _check(lib().episdet_search_batched(ds, os_, n, rs))
+    return [_to_result(os_[i].order, rs[i], keep[i]) for i in range(n)]
+
+
+def search_perm(planes, num_samples: int, labels, *, order: int = 2, score="k2", top_k: int = 1024, device: int = 0,
+                engine="auto") -> list:
+    pp, mp = _ptr(planes)
+    pl, ml = _ptr(labels)
+    if mp != ml:
+        raise TypeError("planes and labels must live in the same memory")
+    nl = int(labels.shape[0])
+    c = Cohort(pp, int(planes.shape[0]), num_samples, mp)
+    o = make_options(order, score, top_k, device, engine)
+    rs = (Result * nl)()
+    keep = []
+    for i in range(nl):
+        r, bufs = _result_buffers(top_k)
+        rs[i] = r
+        keep.append(bufs)
+    _check(lib().episdet_search_perm(ctypes.byref(c), ctypes.c_void_p(pl), nl, ctypes.byref(o), rs))
+    return [_to_result(order, rs[i], keep[i]) for i in range(nl)]
+
+
+def EpistasisDetectionSearch(datasetCases, datasetControls, numSNPs, numCases, numControls, numSNPsWithPadding,
+                             numCasesWithPadding, numControlsWithPadding, *, triplets=True, mi_score=False):
+    """The reference's entry point (src/search-triplets.cu:8): returns
+    (status, roundsCounter, searchTime, outputFromGpu, packedIndices).
+
+    status is 0 on success like cudaSuccess; the padded sizes must be the ones
+    the reference's loader computes (src/tensor-episdet.cu:87-95)."""
+    if numCasesWithPadding != class_words(numCases) * 32 or numControlsWithPadding != class_words(numControls) * 32 \
+            or numSNPsWithPadding < numSNPs:
+        return 1, 0, 0.0, 0.0, 0
+    try:
+        r = search(datasetCases, datasetControls, numCases, numControls, num_snps=numSNPs,
+                   order=3 if triplets else 2, score="mi" if mi_score else "k2")
+    except EpisdetError as e:
+        return e.status, 0, 0.0, 0.0, 0
+    return 0, r.rounds, r.seconds, float(np.float32(r.score)), r.packed_indices

@@ -1,0 +1,153 @@
+"""CPU oracle against the known-answer fixtures and algebraic invariants.
+
+The fixtures (tests/golden/known_answers.json, written by
+tests/golden/make_golden.py) count every contingency table directly from the
+genotype matrix and score it with include/scoring.hpp's formulas in plain
+Python, independently of the oracle's AND-count + derivation route
+(src/helper.cu:480-548, :634-662).
+"""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "known_answers.json")
+
+
+def _cases():
+    with open(GOLDEN) as f:
+        return json.load(f)["cases"]
+
+
+CASES = _cases()
+
+
+def _planes(oracle, c):
+    return (oracle.pack(np.array(c["cases"])), oracle.pack(np.array(c["controls"])), c["num_cases"],
+            c["num_controls"])
+
+
+def test_pack_roundtrip(oracle):
+    rng = np.random.default_rng(1)
+    for n in (1, 31, 32, 33, 1023, 1024, 1025):
+        g = rng.integers(0, 3, size=(5, n))
+        p = oracle.pack(g)
+        assert p.shape == (5, 2, oracle.class_words(n))
+        assert np.array_equal(oracle.unpack(p, n), g)
+        assert oracle.validate(p, n)
+
+
+def test_msb_first_bit_order(oracle):
+    # Sample 0 is the most significant bit of word 0 (src/helper.cu:72-73 masks the low bits).
+    g = np.full((1, 33), 2)
+    g[0, 0] = 0
+    g[0, 32] = 1
+    p = oracle.pack(g)
+    assert p[0, 0, 0] == 0x80000000 and p[0, 1, 1] == 0x80000000
+
+
+@pytest.mark.parametrize("c", CASES, ids=[c["name"] for c in CASES])
+def test_tables_match_direct_count(oracle, c):
+    cases, controls, nc, nn = _planes(oracle, c)
+    for t in c["tables"]:
+        if c["order"] == 2:
+            cs, cn = oracle.table2(cases, controls, nc, nn, *t["snps"])
+        else:
+            cs, cn = oracle.table3(cases, controls, nc, nn, *t["snps"])
+        assert cs.tolist() == t["cases"], t["snps"]
+        assert cn.tolist() == t["controls"], t["snps"]
+        assert cs.sum() == nc and cn.sum() == nn
+        assert (cs >= 0).all() and (cn >= 0).all()
+
+
+@pytest.mark.parametrize("c", CASES, ids=[c["name"] for c in CASES])
+@pytest.mark.parametrize("score", ["k2", "mi"])
+def test_search_best_matches_fixture(oracle, c, score):
+    cases, controls, nc, nn = _planes(oracle, c)
+    r = oracle.search(cases, controls, nc, nn, order=c["order"], score=score, top_k=64, threads=4)
+    M = len(c["cases"])
+    assert r["sets"] == math.comb(M, c["order"])
+    want = c["best_" + score]
+    assert list(r["best"]) == want["snps"]
+    assert r["best_fp64"] == pytest.approx(want["score"], rel=1e-12, abs=1e-12)
+    # FP64 scores of the fixture's top sets, recomputed by the oracle.
+    by_set = {tuple(s): v for s, v in zip(r["top"], r["top_fp64"])}
+    for e in c["top_" + score][:5]:
+        if tuple(e["snps"]) in by_set:
+            assert by_set[tuple(e["snps"])] == pytest.approx(e["score"], rel=1e-12, abs=1e-12)
+
+
+@pytest.mark.parametrize("c", CASES[:4], ids=[c["name"] for c in CASES[:4]])
+def test_top_list_is_sorted_and_complete(oracle, c):
+    cases, controls, nc, nn = _planes(oracle, c)
+    M = len(c["cases"])
+    total = math.comb(M, c["order"])
+    r = oracle.search(cases, controls, nc, nn, order=c["order"], score="k2", top_k=total + 5, threads=3)
+    assert len(r["top"]) == total
+    f = r["top_fp32"]
+    assert all(f[i] <= f[i + 1] for i in range(len(f) - 1))
+    assert len(set(r["top"])) == total
+
+
+def test_planted_triplet_found(oracle):
+    c = next(x for x in CASES if x["name"].startswith("planted"))
+    cases, controls, nc, nn = _planes(oracle, c)
+    for score in ("k2", "mi"):
+        r = oracle.search(cases, controls, nc, nn, order=3, score=score, top_k=8)
+        assert tuple(r["best"]) == (3, 7, 10)
+
+
+def test_thread_count_does_not_change_answer(oracle):
+    c = CASES[-1]
+    cases, controls, nc, nn = _planes(oracle, c)
+    a = oracle.search(cases, controls, nc, nn, order=2, score="k2", top_k=50, threads=1)
+    b = oracle.search(cases, controls, nc, nn, order=2, score="k2", top_k=50, threads=7)
+    assert a["top"] == b["top"] and a["best"] == b["best"]
+    assert np.array_equal(a["top_fp32"], b["top_fp32"])
+
+
+def test_slab_partitions_the_search(oracle):
+    c = next(x for x in CASES if x["name"] == "tiny_triplets")
+    cases, controls, nc, nn = _planes(oracle, c)
+    M = len(c["cases"])
+    full = oracle.search(cases, controls, nc, nn, order=3, score="k2", top_k=100)
+    parts = [oracle.search(cases, controls, nc, nn, order=3, score="k2", top_k=100, first_begin=a, first_end=a + 1)
+             for a in range(M - 2)]
+    assert sum(p["sets"] for p in parts) == full["sets"]
+    merged = sorted(((float(v), s) for p in parts for s, v in zip(p["top"], p["top_fp64"])))
+    assert merged[0][1] == tuple(full["best"])
+
+
+def test_validate_rejects_bad_planes(oracle):
+    g = np.random.default_rng(3).integers(0, 3, size=(4, 40))
+    p = oracle.pack(g)
+    assert oracle.validate(p, 40)
+    bad = p.copy()
+    bad[1, 0, 1] |= 1  # sample 63: beyond n = 40 -> padding bit
+    assert not oracle.validate(bad, 40)
+    bad = p.copy()
+    bad[2, 0, 0] |= p[2, 1, 0] | 0x80000000
+    bad[2, 1, 0] |= 0x80000000  # sample 0 in both planes
+    assert not oracle.validate(bad, 40)
+
+
+def test_label_split_matches_repacked_classes(oracle):
+    rng = np.random.default_rng(7)
+    n = 77
+    g = rng.integers(0, 3, size=(6, n))
+    lab = rng.random(n) < 0.4
+    label = oracle.pack(np.where(lab, 0, 2)[None, :])[0, 0]
+    cases, controls, nc, nn = oracle.split_by_label(oracle.pack(g), n, label)
+    assert nc == lab.sum() and nn == n - lab.sum()
+    assert np.array_equal(cases, oracle.pack(g[:, lab]))
+    assert np.array_equal(controls, oracle.pack(g[:, ~lab]))
+
+
+def test_fp32_error_is_small(oracle):
+    c = next(x for x in CASES if x["name"].startswith("edge_triplets_1025"))
+    cases, controls, nc, nn = _planes(oracle, c)
+    r = oracle.search(cases, controls, nc, nn, order=3, score="k2", top_k=35)
+    rel = np.abs(r["top_fp32"].astype(np.float64) - r["top_fp64"]) / np.abs(r["top_fp64"])
+    assert rel.max() < 1e-5

@@ -1,0 +1,173 @@
+"""GPU engines against the CPU oracle, through the C-ABI.
+
+Bar: the best set, the FP32 candidate list (sets and FP32 score bits) and the
+FP64 re-scores are identical to the oracle's, because every count is exact
+and both sides evaluate the same score tables with the same operation order.
+"""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = json.load(open(os.path.join(ROOT, "tests", "golden", "known_answers.json")))["cases"]
+ENGINES = ["simt", "tensor"]
+
+
+def assert_same(r, o, k):
+    assert tuple(r.snps) == tuple(o["best"])
+    assert r.score == o["best_fp64"]
+    n = min(k, len(o["top"]))
+    assert [tuple(s) for s in r.top_snps[:n]] == [tuple(s) for s in o["top"][:n]]
+    assert np.array_equal(r.top_fp32[:n].view(np.uint32), o["top_fp32"][:n].view(np.uint32))
+    assert np.array_equal(r.top_fp64[:n], o["top_fp64"][:n])
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+@pytest.mark.parametrize("score", ["k2", "mi"])
+@pytest.mark.parametrize("c", GOLDEN, ids=[c["name"] for c in GOLDEN])
+def test_known_answers(episdet, oracle, c, score, engine):
+    cases, controls = oracle.pack(np.array(c["cases"])), oracle.pack(np.array(c["controls"]))
+    nc, nn = c["num_cases"], c["num_controls"]
+    k = 64
+    r = episdet.search(cases, controls, nc, nn, order=c["order"], score=score, top_k=k, engine=engine)
+    o = oracle.search(cases, controls, nc, nn, order=c["order"], score=score, top_k=k)
+    assert_same(r, o, k)
+    assert list(r.snps) == c["best_" + score]["snps"]
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+@pytest.mark.parametrize("order,M,nc,nn", [(2, 200, 3000, 2500), (3, 60, 700, 1300), (2, 70, 1, 4097),
+                                           (3, 40, 31, 1025), (3, 45, 4097, 33), (2, 129, 1023, 1024)])
+@pytest.mark.parametrize("score", ["k2", "mi"])
+def test_random_datasets(episdet, oracle, order, M, nc, nn, score, engine):
+    cases, controls = episdet.generate(100 + M + nc, M, nc, nn)
+    k = 256
+    r = episdet.search(cases, controls, nc, nn, order=order, score=score, top_k=k, engine=engine)
+    o = oracle.search(cases, controls, nc, nn, order=order, score=score, top_k=k)
+    assert_same(r, o, k)
+    assert r.sets_evaluated == o["sets"]
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_config1_pairs_k2(episdet, oracle, engine):
+    """512 SNPs x 4,096 samples (2,048 + 2,048), independent labels, 2-way K2."""
+    cases, controls = episdet.generate(0xE916, 512, 2048, 2048, maf=(0.05, 0.5))
+    r = episdet.search(cases, controls, 2048, 2048, order=2, score="k2", top_k=1024, engine=engine)
+    o = oracle.search(cases, controls, 2048, 2048, order=2, score="k2", top_k=1024)
+    assert_same(r, o, 1024)
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_planted_triplet(episdet, oracle, engine):
+    cases, controls = episdet.generate(0xE917, 96, 8192, 8192, planted=[(5, 40, 77)], base_risk=0.5, effect=0.25)
+    r = episdet.search(cases, controls, 8192, 8192, order=3, score="k2", top_k=512, engine=engine)
+    assert tuple(r.snps) == (5, 40, 77)
+    o = oracle.search(cases, controls, 8192, 8192, order=3, score="k2", top_k=512)
+    assert_same(r, o, 512)
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+@pytest.mark.parametrize("order", [2, 3])
+def test_slab(episdet, oracle, order, engine):
+    cases, controls = episdet.generate(77, 90, 1500, 1600)
+    r = episdet.search(cases, controls, 1500, 1600, order=order, top_k=128, first_begin=17, first_end=41,
+                       engine=engine)
+    o = oracle.search(cases, controls, 1500, 1600, order=order, top_k=128, first_begin=17, first_end=41)
+    assert_same(r, o, 128)
+
+
+def test_engines_agree(episdet):
+    cases, controls = episdet.generate(5, 150, 2500, 2600)
+    a = episdet.search(cases, controls, 2500, 2600, order=3, top_k=1024, engine="simt")
+    b = episdet.search(cases, controls, 2500, 2600, order=3, top_k=1024, engine="tensor")
+    assert a.snps == b.snps and a.score == b.score
+    assert np.array_equal(a.top_snps, b.top_snps)
+    assert np.array_equal(a.top_fp32.view(np.uint32), b.top_fp32.view(np.uint32))
+
+
+def test_device_resident_inputs(episdet):
+    import torch
+
+    cases, controls = episdet.generate(8, 64, 3000, 2000)
+    h = episdet.search(cases, controls, 3000, 2000, order=3, top_k=64)
+    dc = torch.from_numpy(cases.view(np.int32)).cuda()
+    dn = torch.from_numpy(controls.view(np.int32)).cuda()
+    d = episdet.search(dc, dn, 3000, 2000, num_snps=64, order=3, top_k=64)
+    assert h.snps == d.snps and h.score == d.score and np.array_equal(h.top_snps, d.top_snps)
+
+
+def test_repeat_is_deterministic(episdet):
+    cases, controls = episdet.generate(9, 120, 2000, 2000)
+    a = episdet.search(cases, controls, 2000, 2000, order=2, score="mi", top_k=300)
+    b = episdet.search(cases, controls, 2000, 2000, order=2, score="mi", top_k=300)
+    assert np.array_equal(a.top_snps, b.top_snps) and np.array_equal(a.top_fp64, b.top_fp64)
+
+
+def test_invalid_planes_rejected(episdet):
+    cases, controls = episdet.generate(3, 20, 100, 100)
+    bad = cases.copy()
+    bad[4, 1, 3] |= 1  # a padding bit (sample 127 >= 100)
+    with pytest.raises(episdet.EpisdetError) as e:
+        episdet.search(bad, controls, 100, 100, order=2)
+    assert e.value.name == "EPISDET_ERR_INVALID_INPUT"
+    bad = controls.copy()
+    bad[7, 0, 0] |= 0x80000000
+    bad[7, 1, 0] |= 0x80000000  # sample 0 in both planes
+    with pytest.raises(episdet.EpisdetError):
+        episdet.search(cases, bad, 100, 100, order=3)
+    # the context is still usable afterwards
+    r = episdet.search(cases, controls, 100, 100, order=2, top_k=8)
+    assert len(r.snps) == 2
+
+
+def test_permutations_match_split_searches(episdet, oracle):
+    n, M = 3000, 80
+    planes = episdet.generate_cohort(21, M, n)
+    labels = episdet.generate_labels(22, n, 1400, 4)
+    res = episdet.search_perm(planes, n, labels, order=2, score="k2", top_k=64)
+    for lab, r in zip(labels, res):
+        cases, controls, nc, nn = oracle.split_by_label(planes, n, lab)
+        o = oracle.search(cases, controls, nc, nn, order=2, score="k2", top_k=64)
+        assert_same(r, o, 64)
+
+
+def test_batched_equals_plain(episdet):
+    rng = np.random.default_rng(4)
+    cohorts, opts = [], []
+    for i in range(6):
+        M = int(rng.integers(30, 90))
+        nc, nn = int(rng.integers(500, 3000)), int(rng.integers(500, 3000))
+        c, k = episdet.generate(1000 + i, M, nc, nn)
+        cohorts.append((c, k, nc, nn))
+        opts.append({"order": 2 + i % 2, "score": "k2", "top_k": 32})
+    batched = episdet.search_batched(cohorts, opts)
+    for (c, k, nc, nn), opt, b in zip(cohorts, opts, batched):
+        p = episdet.search(c, k, nc, nn, **opt)
+        assert p.snps == b.snps and p.score == b.score
+        assert np.array_equal(p.top_snps, b.top_snps)
+
+
+@pytest.mark.parametrize("variant,order,score", [("pairs.k2", 2, "k2"), ("triplets.mi", 3, "mi"),
+                                                 ("triplets.k2", 3, "k2"), ("pairs.mi", 2, "mi")])
+def test_cli_output(episdet, oracle, tmp_path, variant, order, score):
+    cases, controls = episdet.generate(31, 70, 1800, 1300)
+    path = str(tmp_path / "data.txt")
+    episdet.write_dataset(path, cases, controls, 1800, 1300)
+    exe = os.path.join(ROOT, "tensor-episdet_b200", "bin", f"tensor-episdet.{variant}.bin")
+    p = subprocess.run([exe, path], capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr
+    lines = p.stdout.splitlines()
+    assert lines[0] == "Num. SNPs: 70" and lines[1] == "Num. Blocks of SNPs: 1"
+    assert lines[2] == "Num. Cases: 1800" and lines[3] == "Num. Controls: 1300"
+    assert "Outer loop iteration 0 out of 1" in lines
+    best = [l for l in lines if "SCORE\t->\t{" in l][0]
+    o = oracle.search(cases, controls, 1800, 1300, order=order, score=score, top_k=16)
+    want = "{" + ", ".join(str(v) for v in o["best"]) + "}: " + f"{np.float32(o['best_fp64']):.6f}"
+    assert best.endswith(want), (best, want)
+    assert "Num. of rounds processed: %d" % (1 if order == 2 else 70) in lines  # BLOCK_SIZE 256 rounds
+    assert any(l.startswith("Unique sets of SNPs evaluated (k=%d): " % order) for l in lines)
