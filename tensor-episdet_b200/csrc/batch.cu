@@ -127,11 +127,11 @@ extern "C" episdet_status episdet_search_perm(const episdet_cohort* cohort, cons
         gather_columns_kernel<<<(unsigned)((t0 + 255) / 256), 256, 0, w->st>>>(d_planes, 2 * M, W,
                                                                                 (const int*)w->perm_idx.p, nc, Wc,
                                                                                 (uint32_t*)w->perm_cls[0].p);
-        CUDA_TRY(cudaGetLastError());
+        CHECK_LAUNCH();
         gather_columns_kernel<<<(unsigned)((t1 + 255) / 256), 256, 0, w->st>>>(d_planes, 2 * M, W,
                                                                                 (const int*)w->perm_idx.p + nc, nn, Wn,
                                                                                 (uint32_t*)w->perm_cls[1].p);
-        CUDA_TRY(cudaGetLastError());
+        CHECK_LAUNCH();
         episdet_dataset d;
         d.cases = (const uint32_t*)w->perm_cls[0].p;
         d.controls = (const uint32_t*)w->perm_cls[1].p;

@@ -83,6 +83,12 @@ episdet_status get_workspace(int device, Workspace** out) {
         CUDA_TRY(cudaStreamCreateWithFlags(&w->st, cudaStreamNonBlocking));
         CUDA_TRY(cudaEventCreate(&w->e0));
         CUDA_TRY(cudaEventCreate(&w->e1));
+        // Every kernel with more than 48 KB of dynamic shared memory, once per device.
+        CUDA_TRY(cudaFuncSetAttribute(search2_simt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSimtSmem2));
+        CUDA_TRY(cudaFuncSetAttribute(search3_simt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSimtSmem3));
+        CUDA_TRY(cudaFuncSetAttribute(merge_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMergeSmem));
+        episdet_status st = tensor_init_attributes();
+        if (st != EPISDET_OK) return st;
         g_ws[device] = w;
     }
     *out = g_ws[device];
@@ -181,10 +187,12 @@ episdet_status stage_dataset(Workspace* w, const episdet_dataset* d, bool valida
     }
     CUDA_TRY(w->flag.ensure(sizeof(int) * 4));
     CUDA_TRY(cudaMemsetAsync(w->flag.p, 0, sizeof(int) * 4, w->st));
+    CUDA_TRY(w->tensor_flag.ensure(sizeof(int) * 4));
+    CUDA_TRY(cudaMemsetAsync(w->tensor_flag.p, 0, sizeof(int) * 4, w->st));
     int warps = 2 * d->num_snps;
     marginals_kernel<<<(warps * 32 + 255) / 256, 256, 0, w->st>>>(*D, (int*)w->marg[0].p, (int*)w->marg[1].p,
                                                                    (int*)w->flag.p);
-    CUDA_TRY(cudaGetLastError());
+    CHECK_LAUNCH();
     ++*launches;
     if (validate) {
         int bad = 0;
@@ -220,13 +228,6 @@ static episdet_status run_simt(Workspace* w, const DevData& D0, const ScoreTable
     DevData D = D0;
     const int M = D.M;
     const int nt = (M + kSimtTileSnps - 1) / kSimtTileSnps;
-    static bool attr_done[64] = {};
-    if (!attr_done[w->device]) {
-        CUDA_TRY(cudaFuncSetAttribute(search2_simt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSimtSmem2));
-        CUDA_TRY(cudaFuncSetAttribute(search3_simt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSimtSmem3));
-        CUDA_TRY(cudaFuncSetAttribute(merge_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMergeSmem));
-        attr_done[w->device] = true;
-    }
     int per_sm = 0;
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search3_simt_kernel, kSimtBlockThreads, kSimtSmem3));
     int grid = w->sms * std::max(per_sm, 1);
@@ -244,7 +245,7 @@ static episdet_status run_simt(Workspace* w, const DevData& D0, const ScoreTable
             for (int i = 0; i < bs_lines; ++i) printf("Outer loop iteration %d out of %d\n", i, bs_lines);
         search2_simt_kernel<<<grid, kSimtBlockThreads, kSimtSmem2, w->st>>>(
             D, T, (const int2*)w->tiles.p, (int)tiles.size(), fb, fe, *S, 0, nullptr, nullptr);
-        CUDA_TRY(cudaGetLastError());
+        CHECK_LAUNCH();
         ++*launches;
         return EPISDET_OK;
     }
@@ -264,7 +265,7 @@ static episdet_status run_simt(Workspace* w, const DevData& D0, const ScoreTable
     CUDA_TRY(cudaMemcpyAsync(d_tiles3, all3.data(), sizeof(int2) * all3.size(), cudaMemcpyHostToDevice, w->st));
     search2_simt_kernel<<<grid, kSimtBlockThreads, kSimtSmem2, w->st>>>(
         D, T, d_pair_tiles, (int)tiles.size(), 0, M, *S, 1, (uint4*)w->pair4[0].p, (uint4*)w->pair4[1].p);
-    CUDA_TRY(cudaGetLastError());
+    CHECK_LAUNCH();
     ++*launches;
     // Per-X launches over the (Y-tile, Z-tile) suffix with Y-tile >= tile(X+1).
     std::vector<int> off((size_t)nt + 1, 0);
@@ -275,7 +276,7 @@ static episdet_status run_simt(Workspace* w, const DevData& D0, const ScoreTable
         int ty0 = (x + 1) / kSimtTileSnps;
         int n3 = off[nt] - off[ty0];
         search3_simt_kernel<<<grid, kSimtBlockThreads, kSimtSmem3, w->st>>>(D, T, x, d_tiles3 + off[ty0], n3, *S);
-        CUDA_TRY(cudaGetLastError());
+        CHECK_LAUNCH();
         ++*launches;
     }
     return EPISDET_OK;
@@ -289,10 +290,10 @@ static episdet_status finish(Workspace* w, const DevData& D, const ScoreTables& 
     CUDA_TRY(w->mcount.ensure(sizeof(int) * 4));
     CUDA_TRY(w->fp64.ensure(sizeof(double) * (size_t)k));
     merge_topk_kernel<<<1, kMergeBlockThreads, kMergeSmem, w->st>>>(S, (Cand*)w->merged.p, (int*)w->mcount.p);
-    CUDA_TRY(cudaGetLastError());
+    CHECK_LAUNCH();
     rescore_kernel<<<(k * 32 + 255) / 256, 256, 0, w->st>>>(D, T, o.order, (const Cand*)w->merged.p,
                                                              (const int*)w->mcount.p, (double*)w->fp64.p, nullptr);
-    CUDA_TRY(cudaGetLastError());
+    CHECK_LAUNCH();
     *launches += 2;
     std::vector<Cand> cands((size_t)k);
     std::vector<double> f64((size_t)k);
@@ -300,8 +301,12 @@ static episdet_status finish(Workspace* w, const DevData& D, const ScoreTables& 
     CUDA_TRY(cudaMemcpyAsync(cands.data(), w->merged.p, sizeof(Cand) * k, cudaMemcpyDeviceToHost, w->st));
     CUDA_TRY(cudaMemcpyAsync(f64.data(), w->fp64.p, sizeof(double) * k, cudaMemcpyDeviceToHost, w->st));
     CUDA_TRY(cudaMemcpyAsync(&cnt, w->mcount.p, sizeof(int), cudaMemcpyDeviceToHost, w->st));
+    int dev_err = 0;
+    CUDA_TRY(cudaMemcpyAsync(&dev_err, w->tensor_flag.p, sizeof(int), cudaMemcpyDeviceToHost, w->st));
     CUDA_TRY(cudaEventRecord(w->e1, w->st));
     CUDA_TRY(cudaStreamSynchronize(w->st));
+    if (dev_err)
+        return set_error(EPISDET_ERR_TIMEOUT, "a bounded device wait gave up (code %d); results discarded", dev_err);
     if (cnt < 1) return set_error(EPISDET_ERR_INTERNAL, "no candidate survived the search");
     const bool maximize = o.score == EPISDET_SCORE_MI;
     int best = 0;

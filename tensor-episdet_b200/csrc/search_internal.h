@@ -20,6 +20,15 @@ episdet_status cuda_fail(cudaError_t e, const char* what);
         if (e_ != cudaSuccess) return cuda_fail(e_, #x); \
     } while (0)
 
+// Launch-error check naming the launch site.
+#define CHECK_LAUNCH()                                                         \
+    do {                                                                       \
+        cudaError_t e_ = cudaGetLastError();                                   \
+        if (e_ != cudaSuccess) return cuda_fail(e_, "launch at " __FILE__ ":" EPI_STR(__LINE__)); \
+    } while (0)
+#define EPI_STR2(x) #x
+#define EPI_STR(x) EPI_STR2(x)
+
 // Grow-only device allocation kept between calls.
 struct DevBuf {
     void* p = nullptr;
@@ -63,6 +72,9 @@ episdet_status check_dataset(const episdet_dataset* d, int order);
 // One search; the caller holds w->mu and has validated the options.
 episdet_status search_locked(Workspace* w, const episdet_dataset* data, const episdet_options& o,
                              episdet_result* result);
+
+// Sets the tensor engine's kernel attributes on the current device.
+episdet_status tensor_init_attributes();
 
 // Tensor-core engine (tensor.cu).  Fills S with the per-CTA candidate lists.
 episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const episdet_options& o, int fb, int fe,

@@ -1,13 +1,717 @@
 // tensor.cu -- tcgen05 (5th-generation tensor core) counting engine.
-#include "search_internal.h"
+//
+// Counting is a matrix product over 0/1 bytes: every {SNP, genotype} bit
+// plane row is unpacked once to bytes, so that for rows a, b the u8 x u8 -> s32
+// product sum_s a[s]*b[s] is the AND-popcount the reference computes as
+// (popc a + popc b - popc(a^b))/2 from its CUTLASS XOR GEMM
+// (src/helper.cu:636-637, :484-485, :714-750).
+//
+// Pipeline per CTA (one CTA per SM, persistent over a tile list):
+//   warp 0      TMA producer: 128x128-byte tiles of the A and B row blocks,
+//               128-byte swizzle, 4-stage mbarrier ring (no multicast).
+//   warp 1      MMA issuer: tcgen05.mma.cta_group::1.kind::i8, M=N=128,
+//               K=32 per instruction, accumulators in TMEM (512 columns).
+//   warps 2..5  epilogue: tcgen05.ld of the counts, derivation of the 9 / 27
+//               contingency cells, K2 / MI score, per-CTA top-K candidates.
+//               No count ever returns to HBM.
+//
+// Tiles are 64 SNPs x 2 planes = 128 rows on both sides; accumulators are
+// kept per K segment:
+//   pairs:    segments {cases, controls}                 -> 2 x 128 columns
+//   triplets: segments {cases, controls} x {X genotype a, X genotype b}
+//                                                        -> 4 x 128 columns
+// For triplets the sample columns are regrouped per first SNP X by X's
+// genotype (xinfo/compact kernels below), keeping the two genotypes of X with
+// the fewest samples; the third is recovered from the Y-Z pair table exactly
+// as the reference recovers genotype 2 (src/helper.cu:494-548).  This replaces
+// the materialised X AND Y operand of src/helper.cu:396-425 and reduces the
+// tensor work per triplet from 8 N to 4 (N - max_g count(X=g)) MACs.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <vector>
+
+#include "common.cuh"
+#include "device_data.cuh"
 #include "host_util.h"
+#include "search_internal.h"
+#include "tc_ptx.cuh"
 
 namespace episdet {
+namespace tc {
+
+constexpr int kTileSnps = 64;
+constexpr int kTileRows = 128;
+constexpr int kKB = 128;  // bytes (samples) per K block
+constexpr int kStages = 4;
+constexpr int kTileBytes = kTileRows * kKB;
+constexpr int kStageBytes = 2 * kTileBytes;
+constexpr int kCap = 4096;
+constexpr int kThreads = 192;
+constexpr int kEpiThreads = 128;
+constexpr int kEpiPerStep = kEpiThreads * 4;
+constexpr uint64_t kWaitLimitNs = 4000000000ull;
+constexpr uint32_t kIdesc = ptx::idesc_u8(128);
+
+enum Mode { kPairsScore = 0, kPairsStore = 1, kTriplets = 2 };
+
+struct Seg {
+    int kb0, kb1;  // K-block range [kb0, kb1)
+};
+
+// Per-X sample regrouping: genotypes ga < gb of X are kept, gd is derived.
+struct XInfo {
+    int gd, ga, gb, pad;
+    int len[2][2];  // [class][kept genotype] samples
+    Seg seg[4];     // [class*2 + kept genotype]
+};
+
+struct TcParams {
+    DevData D;
+    ScoreTables T;
+    Slots S;
+    const int2* tiles;  // (A tile, B tile) in 64-SNP units
+    int ntiles;
+    int mode;
+    int xsnp;
+    const XInfo* xinfo;
+    Seg seg2[2];
+    int first_begin, first_end;
+    uint4* pair_out0;
+    uint4* pair_out1;
+    int* err;
+};
+
+constexpr size_t kSmemTopk = (size_t)kStages * kStageBytes;
+constexpr size_t kSmemBars = kSmemTopk + (size_t)kCap * sizeof(Cand);
+constexpr size_t kSmemMisc = kSmemBars + 16 * sizeof(uint64_t);
+constexpr size_t kSmemTotal = kSmemMisc + 64 + 1024;
+
+// ------------------------------------------------------------ operand prep
+// Packed planes -> 0/1 bytes.  Row r = 2*snp + g holds the cases' bytes in
+// [0, Kc) and the controls' in [Kc, Kc + Kn) of a pitch-Kc+Kn row.
+__global__ void __launch_bounds__(256) unpack_kernel(DevData D, uint8_t* __restrict__ out, int rows, int pitch) {
+    const int Kc = D.W[0] * 32;
+    const int chunks = pitch / 16;
+    long total = (long)rows * chunks;
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+        int r = (int)(t / chunks);
+        int k = (int)(t % chunks) * 16;
+        int c = k < Kc ? 0 : 1;
+        int kk = k - (c ? Kc : 0);
+        uint32_t word = __ldg(D.bits[c] + (size_t)r * D.W[c] + (kk >> 5));
+        uint32_t h = (word >> (16 - (kk & 31))) & 0xFFFFu;
+        uint32_t o[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            uint32_t n = (h >> (12 - 4 * e)) & 0xFu;  // 4 samples, first sample in bit 3
+            o[e] = ((n >> 3) & 1u) | ((n << 6) & 0x100u) | ((n << 15) & 0x10000u) | ((n << 24) & 0x1000000u);
+        }
+        *reinterpret_cast<uint4*>(out + (size_t)r * pitch + k) = make_uint4(o[0], o[1], o[2], o[3]);
+    }
+}
+
+// Block-wide exclusive scan of one int per thread (blockDim.x = 1024).
+__device__ __forceinline__ int block_exclusive_scan(int v, int* s_warp, int* total) {
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int w = lane < (int)(blockDim.x >> 5) ? s_warp[lane] : 0;
+        int z = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xFFFFFFFFu, z, o);
+            if (lane >= o) z += y;
+        }
+        s_warp[lane] = z - w;
+        if (lane == 31) *total = z;
+    }
+    __syncthreads();
+    int r = s_warp[warp] + x - v;
+    __syncthreads();
+    return r;
+}
+
+// Per first SNP X and class: which genotype of X to derive (the most frequent
+// over both classes), and the ascending sample indices of the two kept ones.
+__global__ void __launch_bounds__(1024) xinfo_kernel(DevData D, int X, XInfo* info, int* idx, int max_n) {
+    __shared__ int s_warp[32];
+    __shared__ int s_total;
+    const int c = blockIdx.x;
+    const int M = D.M;
+    int tot[3];
+#pragma unroll
+    for (int g = 0; g < 3; ++g) tot[g] = __ldg(D.marg[0] + g * M + X) + __ldg(D.marg[1] + g * M + X);
+    int gd = 0;
+    if (tot[1] > tot[gd]) gd = 1;
+    if (tot[2] > tot[gd]) gd = 2;
+    const int ga = gd == 0 ? 1 : 0, gb = gd == 2 ? 1 : 2;
+    const int W = D.W[c], n = D.n[c];
+    const uint32_t* p0 = D.bits[c] + (size_t)X * 2 * W;
+    const uint32_t* p1 = p0 + W;
+    const int per = (W + blockDim.x - 1) / blockDim.x;
+    const int w0 = threadIdx.x * per, w1 = min(W, w0 + per);
+    const int base_kb = c == 0 ? 0 : (D.W[0] * 32 + 256) / kKB;
+    int kb = base_kb;
+    for (int s = 0; s < 2; ++s) {
+        const int g = s == 0 ? ga : gb;
+        int cnt = 0;
+        for (int w = w0; w < w1; ++w) {
+            uint32_t m = g == 0 ? p0[w] : (g == 1 ? p1[w] : ~(p0[w] | p1[w]));
+            int lo = w * 32;
+            uint32_t valid = (lo + 32 <= n) ? 0xFFFFFFFFu : (lo >= n ? 0u : (0xFFFFFFFFu << (32 - (n - lo))));
+            cnt += __popc(m & valid);
+        }
+        int off = block_exclusive_scan(cnt, s_warp, &s_total);
+        int* out = idx + ((size_t)c * 2 + s) * max_n;
+        for (int w = w0; w < w1; ++w) {
+            uint32_t m = g == 0 ? p0[w] : (g == 1 ? p1[w] : ~(p0[w] | p1[w]));
+            int lo = w * 32;
+            uint32_t valid = (lo + 32 <= n) ? 0xFFFFFFFFu : (lo >= n ? 0u : (0xFFFFFFFFu << (32 - (n - lo))));
+            m &= valid;
+            while (m) {
+                int lz = __clz(m);
+                out[off++] = lo + lz;
+                m &= ~(0x80000000u >> lz);
+            }
+        }
+        int len = s_total;
+        if (threadIdx.x == 0) {
+            info->len[c][s] = len;
+            info->seg[c * 2 + s].kb0 = kb;
+            info->seg[c * 2 + s].kb1 = kb + (len + kKB - 1) / kKB;
+        }
+        kb += (len + kKB - 1) / kKB;
+        __syncthreads();
+    }
+    if (c == 0 && threadIdx.x == 0) {
+        info->gd = gd;
+        info->ga = ga;
+        info->gb = gb;
+        info->pad = 0;
+    }
+}
+
+// Regrouped operand rows for one X: row r, class c, segment s holds byte
+// bit(r, idx[c][s][k]) at column seg.kb0*128 + k (zero past the segment's
+// length up to its 128-byte end).  Rows below row0 are not needed by X.
+__global__ void __launch_bounds__(256) compact_kernel(DevData D, const XInfo* __restrict__ info,
+                                                      const int* __restrict__ idx, int max_n, int row0, int rows,
+                                                      uint8_t* __restrict__ out, int pitch) {
+    const int cmax0 = (D.W[0] * 32 + 256) / 16, cmax1 = (D.W[1] * 32 + 256) / 16;
+    const int chunks = cmax0 + cmax1;
+    const long total = (long)rows * chunks;
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+        int r = row0 + (int)(t / chunks);
+        int ch = (int)(t % chunks);
+        int c = ch < cmax0 ? 0 : 1;
+        int k = (ch - (c ? cmax0 : 0)) * 16;
+        int la = info->len[c][0], lb = info->len[c][1];
+        int pa = ((la + kKB - 1) / kKB) * kKB, pb = ((lb + kKB - 1) / kKB) * kKB;
+        if (k >= pa + pb) continue;
+        int s = k < pa ? 0 : 1;
+        int kk = k - (s ? pa : 0);
+        int len = s ? lb : la;
+        const int* ix = idx + ((size_t)c * 2 + s) * max_n;
+        const uint32_t* src = D.bits[c] + (size_t)r * D.W[c];
+        uint32_t o[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+            if (kk + e < len) {
+                int j = __ldg(ix + kk + e);
+                uint32_t bit = (__ldg(src + (j >> 5)) >> (31 - (j & 31))) & 1u;
+                o[e >> 2] |= bit << (8 * (e & 3));
+            }
+        }
+        int col = info->seg[c * 2 + s].kb0 * kKB + kk;
+        *reinterpret_cast<uint4*>(out + (size_t)r * pitch + col) = make_uint4(o[0], o[1], o[2], o[3]);
+    }
+}
+
+__device__ __forceinline__ void record_error(int* err, int code) { atomicCAS(err, 0, code); }
+
+// ------------------------------------------------------------------ kernel
+__global__ void __launch_bounds__(kThreads, 1)
+    tc_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ TcParams P) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* stages = smem;
+    Cand* tbuf = reinterpret_cast<Cand*>(smem + kSmemTopk);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kSmemBars);
+    uint64_t* full = bars;
+    uint64_t* empty = bars + kStages;
+    uint64_t* tfull = bars + 2 * kStages;
+    uint64_t* tempty = bars + 2 * kStages + 2;
+    uint64_t* drain = bars + 2 * kStages + 4;
+    uint32_t* s_tmem = reinterpret_cast<uint32_t*>(smem + kSmemMisc);
+    int* s_abort = reinterpret_cast<int*>(smem + kSmemMisc + 4);
+    int* s_never = reinterpret_cast<int*>(smem + kSmemMisc + 8);  // stays 0: drain waits ignore aborts
+    int* s_epi_fail = reinterpret_cast<int*>(smem + kSmemMisc + 12);
+    int* s_count = reinterpret_cast<int*>(smem + kSmemMisc + 16);
+    Cand* s_thr = reinterpret_cast<Cand*>(smem + kSmemMisc + 32);
+    volatile int* abort = s_abort;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int mode = P.mode;
+    int nseg = 2;
+    Seg seg[4];
+    int ga = 0, gb = 1;
+    if (mode == kTriplets) {
+        nseg = 4;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) seg[s] = P.xinfo->seg[s];
+        ga = P.xinfo->ga;
+        gb = P.xinfo->gb;
+    } else {
+        seg[0] = P.seg2[0];
+        seg[1] = P.seg2[1];
+        seg[2] = seg[3] = Seg{0, 0};
+    }
+    const int nbuf = 4 / nseg;
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < kStages; ++i) {
+            ptx::mbar_init(&full[i], 1);
+            ptx::mbar_init(&empty[i], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            ptx::mbar_init(&tfull[b], 1);
+            ptx::mbar_init(&tempty[b], kEpiThreads);
+        }
+        ptx::mbar_init(drain, 1);
+        *s_abort = 0;
+        *s_never = 0;
+        *s_epi_fail = 0;
+        ptx::fence_barrier_init();
+    }
+    if (warp == 1) {
+        ptx::tmem_alloc(s_tmem, 512);
+        ptx::tmem_relinquish();
+    }
+    if (warp == 0 && lane == 0) ptx::prefetch_tmap(&tmap);
+    ptx::tc_fence_before();
+    __syncthreads();
+    ptx::tc_fence_after();
+    const uint32_t tmem = *s_tmem;
+
+    if (warp == 0) {
+        // ---------------------------------------------------- TMA producer
+        if (lane == 0) {
+            uint32_t stage = 0, phase = 0;
+            uint32_t pend_phase[kStages];
+            bool pend[kStages];
+#pragma unroll
+            for (int i = 0; i < kStages; ++i) {
+                pend[i] = false;
+                pend_phase[i] = 0;
+            }
+            bool ok = true;
+            for (int t = blockIdx.x; ok && t < P.ntiles; t += gridDim.x) {
+                const int2 tl = P.tiles[t];
+                for (int s = 0; ok && s < nseg; ++s)
+                    for (int kb = seg[s].kb0; kb < seg[s].kb1; ++kb) {
+                        if (!ptx::mbar_wait(&empty[stage], phase ^ 1, abort, kWaitLimitNs)) {
+                            ok = false;
+                            break;
+                        }
+                        ptx::mbar_arrive_expect_tx(&full[stage], kStageBytes);
+                        uint8_t* sa = stages + (size_t)stage * kStageBytes;
+                        ptx::tma_load_2d(sa, &tmap, kb * kKB, tl.x * kTileRows, &full[stage]);
+                        ptx::tma_load_2d(sa + kTileBytes, &tmap, kb * kKB, tl.y * kTileRows, &full[stage]);
+                        pend[stage] = true;
+                        pend_phase[stage] = phase;
+                        if (++stage == kStages) {
+                            stage = 0;
+                            phase ^= 1;
+                        }
+                    }
+            }
+            if (!ok) {
+                record_error(P.err, 1);
+                *s_abort = 1;
+            }
+            // Never leave with a copy in flight.
+            for (int i = 0; i < kStages; ++i)
+                if (pend[i] && !ptx::mbar_wait(&full[i], pend_phase[i], s_never, kWaitLimitNs))
+                    record_error(P.err, 2);
+        }
+    } else if (warp == 1) {
+        // ---------------------------------------------------- MMA issuer
+        if (lane == 0) {
+            uint32_t stage = 0, phase = 0;
+            bool ok = true;
+            int local = 0;
+            for (int t = blockIdx.x; ok && t < P.ntiles; t += gridDim.x, ++local) {
+                const int b = local % nbuf;
+                const uint32_t use = (uint32_t)(local / nbuf);
+                if (!ptx::mbar_wait(&tempty[b], (use & 1) ^ 1, abort, kWaitLimitNs)) {
+                    ok = false;
+                    break;
+                }
+                ptx::tc_fence_after();
+                const uint32_t dbase = tmem + (uint32_t)(b * nseg * 128);
+                for (int s = 0; ok && s < nseg; ++s)
+                    for (int kb = seg[s].kb0; kb < seg[s].kb1; ++kb) {
+                        if (!ptx::mbar_wait(&full[stage], phase, abort, kWaitLimitNs)) {
+                            ok = false;
+                            break;
+                        }
+                        ptx::tc_fence_after();
+                        const uint32_t sa = ptx::smem_u32(stages + (size_t)stage * kStageBytes);
+                        const uint64_t ad = ptx::smem_desc_sw128(sa), bd = ptx::smem_desc_sw128(sa + kTileBytes);
+#pragma unroll
+                        for (int kk = 0; kk < kKB / 32; ++kk)
+                            ptx::mma_u8(dbase + (uint32_t)(s * 128), ad + 2 * kk, bd + 2 * kk, kIdesc,
+                                        (kb > seg[s].kb0 || kk > 0) ? 1u : 0u);
+                        ptx::mma_commit(&empty[stage]);
+                        if (++stage == kStages) {
+                            stage = 0;
+                            phase ^= 1;
+                        }
+                    }
+                if (ok) ptx::mma_commit(&tfull[b]);
+            }
+            if (!ok) {
+                record_error(P.err, 3);
+                *s_abort = 1;
+            }
+            // Every MMA this thread issued completes before TMEM is released.
+            ptx::mma_commit(drain);
+            if (!ptx::mbar_wait(drain, 0, s_never, kWaitLimitNs))
+                record_error(P.err, 4);
+        }
+    } else {
+        // ---------------------------------------------------- epilogue
+        const int etid = threadIdx.x - 64;
+        const int q = warp & 3;  // TMEM lane quarter this warp may access
+        const int m = q * 32 + lane;
+        const int yl = m >> 1, j_own = m & 1;
+        const int zoff = j_own ? 4 : 0;
+        const BarNamed bar{1, kEpiThreads};
+        const bool maximize = P.T.score == 1;
+        const int M = P.D.M;
+        LocalTopK<kCap, kEpiThreads> tk{tbuf, s_count, s_thr, P.S.k, etid};
+        if (mode != kPairsStore) tk.load(P.S.lists + (size_t)blockIdx.x * P.S.k, P.S.counts[blockIdx.x], bar);
+        bool seg_empty[4];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) seg_empty[s] = seg[s].kb1 <= seg[s].kb0;
+        bool ok = true;
+        int local = 0;
+        for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x, ++local) {
+            const int b = local % nbuf;
+            const uint32_t use = (uint32_t)(local / nbuf);
+            // The decision to leave must be uniform over the 128 epilogue
+            // threads (they meet at named barriers), so it is taken after a
+            // barrier from a flag only they write.
+            if (!ptx::mbar_wait(&tfull[b], use & 1, abort, kWaitLimitNs)) *s_epi_fail = 1;
+            bar();
+            if (*(volatile int*)s_epi_fail) {
+                ok = false;
+                break;
+            }
+            ptx::tc_fence_after();
+            const int2 tl = P.tiles[t];
+            const int arow = tl.x * kTileSnps + yl;  // this thread's A SNP (pairs: a, triplets: Y)
+            const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * nseg * 128);
+            // Per-row constants.
+            int ma[2][3] = {{0, 0, 0}, {0, 0, 0}}, mx[2][3] = {{0, 0, 0}, {0, 0, 0}};
+            int xy9[2][9];
+            const int X = P.xsnp;
+            const bool row_ok = arow < M && (mode != kTriplets || arow > X);
+            if (row_ok) {
+#pragma unroll
+                for (int c = 0; c < 2; ++c) load_marg3(P.D.marg[c], M, arow, ma[c]);
+                if (mode == kTriplets) {
+#pragma unroll
+                    for (int c = 0; c < 2; ++c) {
+                        load_marg3(P.D.marg[c], M, X, mx[c]);
+                        pair9_from4(xy9[c], __ldg(P.D.pair4[c] + (size_t)X * M + arow), mx[c], ma[c]);
+                    }
+                }
+            }
+            for (int ch = 0; ch < 8; ++ch) {
+                uint32_t v[4][16];
+                __syncwarp();
+#pragma unroll
+                for (int s = 0; s < 4; ++s)
+                    if (s < nseg) ptx::tmem_ld16(trow + (uint32_t)(s * 128 + ch * 16), v[s]);
+                ptx::tmem_wait_ld();
+                if (ch == 7) {
+                    ptx::tc_fence_before();
+                    ptx::mbar_arrive(&tempty[b]);
+                }
+#pragma unroll
+                for (int s = 0; s < 4; ++s)
+                    if (s >= nseg || seg_empty[s])
+#pragma unroll
+                        for (int e = 0; e < 16; ++e) v[s][e] = 0;
+                // Partner lane (other plane of the same A SNP) sends the counts of our 4 B SNPs.
+                uint32_t r[4][8];
+#pragma unroll
+                for (int s = 0; s < 4; ++s)
+#pragma unroll
+                    for (int e = 0; e < 8; ++e)
+                        r[s][e] = __shfl_xor_sync(0xFFFFFFFFu, j_own ? v[s][e] : v[s][8 + e], 1);
+                Cand thr = *s_thr;
+#pragma unroll
+                for (int z = 0; z < 4; ++z) {
+                    const int bsnp = tl.y * kTileSnps + ch * 8 + zoff + z;
+                    // cnt(s, jj, kk): A plane jj, B plane kk, segment s
+                    auto cnt = [&](int s, int jj, int kk) -> int {
+                        const uint32_t own = j_own ? v[s][8 + 2 * z + kk] : v[s][2 * z + kk];
+                        return (int)(jj == j_own ? own : r[s][2 * z + kk]);
+                    };
+                    if (mode == kPairsStore) {
+                        if (row_ok && arow < bsnp && bsnp < M) {
+                            size_t o = (size_t)arow * M + bsnp;
+                            P.pair_out0[o] = make_uint4(cnt(0, 0, 0), cnt(0, 0, 1), cnt(0, 1, 0), cnt(0, 1, 1));
+                            P.pair_out1[o] = make_uint4(cnt(1, 0, 0), cnt(1, 0, 1), cnt(1, 1, 0), cnt(1, 1, 1));
+                        }
+                        continue;
+                    }
+                    if (mode == kPairsScore) {
+                        if (!(row_ok && arow < bsnp && bsnp < M && arow >= P.first_begin && arow < P.first_end))
+                            continue;
+                        int cs[9], cn[9], mb[3];
+                        cs[0] = cnt(0, 0, 0);
+                        cs[1] = cnt(0, 0, 1);
+                        cs[3] = cnt(0, 1, 0);
+                        cs[4] = cnt(0, 1, 1);
+                        load_marg3(P.D.marg[0], M, bsnp, mb);
+                        derive9(cs, ma[0], mb);
+                        cn[0] = cnt(1, 0, 0);
+                        cn[1] = cnt(1, 0, 1);
+                        cn[3] = cnt(1, 1, 0);
+                        cn[4] = cnt(1, 1, 1);
+                        load_marg3(P.D.marg[1], M, bsnp, mb);
+                        derive9(cn, ma[1], mb);
+                        float sc = score32<9>(P.T, cs, cn);
+                        Cand cd;
+                        cd.key = score_key(sc, maximize);
+                        cd.pad = 0;
+                        cd.set = set_key2((uint32_t)arow, (uint32_t)bsnp);
+                        tk.offer(cd, thr);
+                        continue;
+                    }
+                    // triplets: X < Y = arow < Z = bsnp
+                    if (!(row_ok && arow < bsnp && bsnp < M)) continue;
+                    int tab[2][27];
+#pragma unroll
+                    for (int c = 0; c < 2; ++c) {
+                        int mz[3], xz9[9], yz9[9];
+                        load_marg3(P.D.marg[c], M, bsnp, mz);
+                        const uint4 yz = __ldg(P.D.pair4[c] + (size_t)arow * M + bsnp);
+                        const int yz4[4] = {(int)yz.x, (int)yz.y, (int)yz.z, (int)yz.w};
+#pragma unroll
+                        for (int jj = 0; jj < 2; ++jj)
+#pragma unroll
+                            for (int kk = 0; kk < 2; ++kk) {
+                                const int g0 = cnt(2 * c, jj, kk), g1 = cnt(2 * c + 1, jj, kk);
+                                const int gdv = yz4[jj * 2 + kk] - g0 - g1;
+                                tab[c][EPI_C3(0, jj, kk)] = ga == 0 ? g0 : (gb == 0 ? g1 : gdv);
+                                tab[c][EPI_C3(1, jj, kk)] = ga == 1 ? g0 : (gb == 1 ? g1 : gdv);
+                            }
+                        pair9_from4(xz9, __ldg(P.D.pair4[c] + (size_t)X * M + bsnp), mx[c], mz);
+                        pair9_from4(yz9, yz, ma[c], mz);
+                        derive27(tab[c], xy9[c], xz9, yz9);
+                    }
+                    float sc = score32<27>(P.T, tab[0], tab[1]);
+                    Cand cd;
+                    cd.key = score_key(sc, maximize);
+                    cd.pad = 0;
+                    cd.set = set_key3((uint32_t)X, (uint32_t)arow, (uint32_t)bsnp);
+                    tk.offer(cd, thr);
+                }
+                if (mode != kPairsStore) {
+                    bar();
+                    if (*s_count > kCap - kEpiPerStep) tk.compact(bar);
+                }
+            }
+        }
+        if (!ok) {
+            record_error(P.err, 5);
+            *s_abort = 1;
+        } else if (mode != kPairsStore) {
+            tk.store(P.S.lists + (size_t)blockIdx.x * P.S.k, P.S.counts + blockIdx.x, bar);
+        }
+    }
+    ptx::tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        ptx::tc_fence_after();
+        ptx::tmem_dealloc(tmem, 512);
+    }
+}
+
+}  // namespace tc
+
+// ------------------------------------------------------------------ host
+using namespace tc;
+
+static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+static episdet_status get_encoder() {
+    if (g_encode) return EPISDET_OK;
+    cudaDriverEntryPointQueryResult q;
+    void* fn = nullptr;
+    cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+    if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+        return set_error(EPISDET_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    return EPISDET_OK;
+}
+
+// rows x pitch bytes, row-major, 128x128-byte boxes, 128-byte swizzle.
+static episdet_status make_tmap(CUtensorMap* m, void* base, uint64_t rows, uint64_t pitch) {
+    cuuint64_t dims[2] = {pitch, rows};
+    cuuint64_t strides[1] = {pitch};
+    cuuint32_t box[2] = {kKB, kTileRows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, base, dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_error(EPISDET_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return EPISDET_OK;
+}
+
+episdet_status tensor_init_attributes() {
+    CUDA_TRY(cudaFuncSetAttribute(tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemTotal));
+    return get_encoder();
+}
+
+static int grid_for(long work, int threads) {
+    long b = (work + threads - 1) / threads;
+    return (int)std::min<long>(std::max<long>(b, 1), 148L * 64);
+}
 
 episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const episdet_options& o, int fb, int fe,
                           Slots* S, uint64_t* launches, bool progress) {
-    (void)w; (void)D; (void)T; (void)o; (void)fb; (void)fe; (void)S; (void)launches; (void)progress;
-    return set_error(EPISDET_ERR_UNSUPPORTED, "tensor engine not built");
+    episdet_status st = get_encoder();
+    if (st != EPISDET_OK) return st;
+    const int M = D.M;
+    const int grid = w->sms;
+    st = prepare_slots(w, grid, o.top_k, S);
+    if (st != EPISDET_OK) return st;
+    CUDA_TRY(w->tensor_flag.ensure(sizeof(int) * 4));
+    int* d_err = (int*)w->tensor_flag.p;
+
+    const int Kc = D.W[0] * 32, Kn = D.W[1] * 32;
+    const int pitch2 = Kc + Kn;
+    const int rows = 2 * M;
+    CUDA_TRY(w->planes8.ensure((size_t)rows * pitch2));
+    uint8_t* P2 = (uint8_t*)w->planes8.p;
+    unpack_kernel<<<grid_for((long)rows * (pitch2 / 16), 256), 256, 0, w->st>>>(D, P2, rows, pitch2);
+    CHECK_LAUNCH();
+    ++*launches;
+    CUtensorMap tm2;
+    st = make_tmap(&tm2, P2, (uint64_t)rows, (uint64_t)pitch2);
+    if (st != EPISDET_OK) return st;
+
+    const int nt = (M + kTileSnps - 1) / kTileSnps;
+    const int bs_lines = (M + 255) / 256;
+    std::vector<int2> tiles;
+    TcParams p;
+    memset(&p, 0, sizeof(p));
+    p.D = D;
+    p.T = T;
+    p.S = *S;
+    p.first_begin = fb;
+    p.first_end = fe;
+    p.err = d_err;
+    p.seg2[0] = Seg{0, Kc / kKB};
+    p.seg2[1] = Seg{Kc / kKB, pitch2 / kKB};
+
+    if (o.order == 2) {
+        for (int a = fb / kTileSnps; a <= (fe - 1) / kTileSnps; ++a)
+            for (int b = a; b < nt; ++b) tiles.push_back(make_int2(a, b));
+        CUDA_TRY(w->tiles.ensure(sizeof(int2) * tiles.size()));
+        CUDA_TRY(cudaMemcpyAsync(w->tiles.p, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice, w->st));
+        if (progress)
+            for (int i = 0; i < bs_lines; ++i) printf("Outer loop iteration %d out of %d\n", i, bs_lines);
+        p.tiles = (const int2*)w->tiles.p;
+        p.ntiles = (int)tiles.size();
+        p.mode = kPairsScore;
+        tc_kernel<<<grid, kThreads, kSmemTotal, w->st>>>(tm2, p);
+        CHECK_LAUNCH();
+        ++*launches;
+        return EPISDET_OK;
+    }
+
+    // 3-way: pair table of every SNP pair whose first index is in a tile >= fb's.
+    for (int c = 0; c < 2; ++c) {
+        CUDA_TRY(w->pair4[c].ensure(sizeof(uint4) * (size_t)M * M));
+        D.pair4[c] = (const uint4*)w->pair4[c].p;
+    }
+    p.D = D;
+    std::vector<int2> ptiles, all3;
+    for (int a = fb / kTileSnps; a < nt; ++a)
+        for (int b = a; b < nt; ++b) ptiles.push_back(make_int2(a, b));
+    for (int a = 0; a < nt; ++a)
+        for (int b = a; b < nt; ++b) all3.push_back(make_int2(a, b));
+    CUDA_TRY(w->tiles.ensure(sizeof(int2) * (ptiles.size() + all3.size())));
+    int2* d_ptiles = (int2*)w->tiles.p;
+    int2* d_all3 = d_ptiles + ptiles.size();
+    CUDA_TRY(cudaMemcpyAsync(d_ptiles, ptiles.data(), sizeof(int2) * ptiles.size(), cudaMemcpyHostToDevice, w->st));
+    CUDA_TRY(cudaMemcpyAsync(d_all3, all3.data(), sizeof(int2) * all3.size(), cudaMemcpyHostToDevice, w->st));
+    p.tiles = d_ptiles;
+    p.ntiles = (int)ptiles.size();
+    p.mode = kPairsStore;
+    p.pair_out0 = (uint4*)w->pair4[0].p;
+    p.pair_out1 = (uint4*)w->pair4[1].p;
+    tc_kernel<<<grid, kThreads, kSmemTotal, w->st>>>(tm2, p);
+    CHECK_LAUNCH();
+    ++*launches;
+
+    // Per-X regrouped operands (double buffered) and their segment tables.
+    const int pitchx = Kc + 256 + Kn + 256;
+    const int max_n = std::max(D.n[0], D.n[1]);
+    for (int i = 0; i < 2; ++i) CUDA_TRY(w->xsub[i].ensure((size_t)rows * pitchx));
+    const size_t info_bytes = 256;
+    const size_t idx_bytes = sizeof(int) * 4 * (size_t)max_n;
+    CUDA_TRY(w->xinfo.ensure(2 * (info_bytes + idx_bytes)));
+    CUtensorMap tmx[2];
+    XInfo* d_info[2];
+    int* d_idx[2];
+    for (int i = 0; i < 2; ++i) {
+        st = make_tmap(&tmx[i], w->xsub[i].p, (uint64_t)rows, (uint64_t)pitchx);
+        if (st != EPISDET_OK) return st;
+        d_info[i] = (XInfo*)((uint8_t*)w->xinfo.p + i * (info_bytes + idx_bytes));
+        d_idx[i] = (int*)((uint8_t*)d_info[i] + info_bytes);
+    }
+    std::vector<int> off((size_t)nt + 1, 0);
+    for (int t = 0; t < nt; ++t) off[t + 1] = off[t] + (nt - t);
+    const int xend = std::min(fe, M - 2);
+    p.mode = kTriplets;
+    for (int x = fb; x < xend; ++x) {
+        if (progress && x % 256 == 0) printf("Outer loop iteration %d out of %d\n", x / 256, bs_lines);
+        const int bi = x & 1;
+        const int t0 = (x + 1) / kTileSnps;
+        xinfo_kernel<<<2, 1024, 0, w->st>>>(D, x, d_info[bi], d_idx[bi], max_n);
+        CHECK_LAUNCH();
+        const int row0 = 2 * t0 * kTileSnps;
+        const int nrows = rows - row0;
+        const long cwork = (long)nrows * ((Kc + 256) / 16 + (Kn + 256) / 16);
+        compact_kernel<<<grid_for(cwork, 256), 256, 0, w->st>>>(D, d_info[bi], d_idx[bi], max_n, row0, nrows,
+                                                                 (uint8_t*)w->xsub[bi].p, pitchx);
+        CHECK_LAUNCH();
+        p.xsnp = x;
+        p.xinfo = d_info[bi];
+        p.tiles = d_all3 + off[t0];
+        p.ntiles = off[nt] - off[t0];
+        tc_kernel<<<grid, kThreads, kSmemTotal, w->st>>>(tmx[bi], p);
+        CHECK_LAUNCH();
+        *launches += 3;
+    }
+    return EPISDET_OK;
 }
 
 }  // namespace episdet
