@@ -65,6 +65,7 @@ enum { EPISDET_ENGINE_AUTO = 0, EPISDET_ENGINE_TENSOR = 1, EPISDET_ENGINE_SIMT =
 /* options.flags */
 #define EPISDET_FLAG_PROGRESS 0x1u     /* print the reference's "Outer loop iteration" lines */
 #define EPISDET_FLAG_NO_VALIDATE 0x2u  /* skip the padding / plane-overlap check */
+#define EPISDET_FLAG_TIMING 0x4u       /* time every counting-kernel launch (result.count_kernel_ms) */
 
 /* One cohort split into cases and controls (the reference's two .bin files). */
 typedef struct episdet_dataset {
@@ -87,13 +88,14 @@ typedef struct episdet_cohort {
 typedef struct episdet_options {
     int32_t order;        /* 2 (pairs) or 3 (triplets) */
     int32_t score;        /* EPISDET_SCORE_K2 (minimised) or EPISDET_SCORE_MI (maximised) */
-    int32_t top_k;        /* FP32 candidates re-scored in FP64; 1..4096, default 1024 */
+    int32_t top_k;        /* FP32 candidates re-scored in FP64; 1..2048, default 1024 */
     int32_t device;       /* CUDA device ordinal, default 0 */
     int32_t engine;       /* EPISDET_ENGINE_* */
     int32_t first_begin;  /* evaluate only sets whose first SNP is in [first_begin, first_end) */
     int32_t first_end;    /* 0 -> num_snps */
     uint32_t flags;       /* EPISDET_FLAG_* */
-    int32_t reserved[8];
+    uint64_t stream;      /* cudaStream_t to run on; 0 = the library's own stream */
+    int32_t reserved[6];
 } episdet_options;
 
 typedef struct episdet_result {
@@ -108,6 +110,11 @@ typedef struct episdet_result {
     double seconds;           /* wall time of the call (the reference's searchTime) */
     double device_ms;         /* device time of the counting+scoring launches */
     uint64_t kernel_launches; /* kernels this call launched */
+    double count_kernel_ms;   /* EPISDET_FLAG_TIMING: summed device time of the counting launches */
+    int64_t count_kernel_launches; /* launches of the counting kernel */
+    double executed_macs;     /* EPISDET_FLAG_TIMING: 8-bit MACs the tensor engine issued (0 for SIMT) */
+    int64_t h2d_bytes;        /* host->device bytes this call copied */
+    int64_t d2h_bytes;        /* device->host bytes this call copied */
     /* Optional caller-owned outputs of capacity top_capacity (may be NULL). */
     int32_t top_capacity;
     uint32_t* top_snps;       /* [top_capacity][3] in FP32 rank order */

@@ -91,6 +91,7 @@ extern "C" episdet_status episdet_search_perm(const episdet_cohort* cohort, cons
     if (st != EPISDET_OK) return st;
     std::lock_guard<std::mutex> lock(w->mu);
     CUDA_TRY(cudaSetDevice(o.device));
+    begin_call(w, o);
     const int W = episdet_class_words(n);
     const size_t plane_words = (size_t)M * 2 * W;
     const uint32_t* d_planes = cohort->planes;

@@ -80,7 +80,8 @@ episdet_status get_workspace(int device, Workspace** out) {
         Workspace* w = new Workspace();
         w->device = device;
         w->sms = prop.multiProcessorCount;
-        CUDA_TRY(cudaStreamCreateWithFlags(&w->st, cudaStreamNonBlocking));
+        CUDA_TRY(cudaStreamCreateWithFlags(&w->own_st, cudaStreamNonBlocking));
+        w->st = w->own_st;
         CUDA_TRY(cudaEventCreate(&w->e0));
         CUDA_TRY(cudaEventCreate(&w->e1));
         // Every kernel with more than 48 KB of dynamic shared memory, once per device.
@@ -93,6 +94,32 @@ episdet_status get_workspace(int device, Workspace** out) {
     }
     *out = g_ws[device];
     return EPISDET_OK;
+}
+
+void begin_call(Workspace* w, const episdet_options& o) {
+    w->st = o.stream ? (cudaStream_t)(uintptr_t)o.stream : w->own_st;
+    w->h2d = w->d2h = 0;
+    w->timing = (o.flags & EPISDET_FLAG_TIMING) != 0;
+    w->tev_used = 0;
+    w->count_launches = 0;
+    w->executed_macs = 0.0;
+}
+
+cudaError_t timer_begin(Workspace* w) {
+    ++w->count_launches;
+    if (!w->timing) return cudaSuccess;
+    while ((int)w->tev.size() < w->tev_used + 2) {
+        cudaEvent_t e;
+        cudaError_t r = cudaEventCreate(&e);
+        if (r != cudaSuccess) return r;
+        w->tev.push_back(e);
+    }
+    return cudaEventRecord(w->tev[w->tev_used++], w->st);
+}
+
+cudaError_t timer_end(Workspace* w) {
+    if (!w->timing) return cudaSuccess;
+    return cudaEventRecord(w->tev[w->tev_used++], w->st);
 }
 
 // Score tables, built on the host in double with glibc (src/search-pairs.cu:83-106):
@@ -131,6 +158,7 @@ episdet_status build_tables(Workspace* w, int score, int nc, int nn, ScoreTables
         CUDA_TRY(cudaMemcpyAsync(w->t32.p, t32.data(), sizeof(float) * size, cudaMemcpyHostToDevice, w->st));
         CUDA_TRY(cudaMemcpyAsync(w->t64.p, t64.data(), sizeof(double) * size, cudaMemcpyHostToDevice, w->st));
         CUDA_TRY(cudaStreamSynchronize(w->st));
+        w->h2d += (int64_t)size * (sizeof(float) + sizeof(double));
         w->tab_score = score;
         w->tab_nc = nc;
         w->tab_nn = nn;
@@ -179,6 +207,7 @@ episdet_status stage_dataset(Workspace* w, const episdet_dataset* d, bool valida
         } else {
             CUDA_TRY(w->bits[c].ensure(bytes));
             CUDA_TRY(cudaMemcpyAsync(w->bits[c].p, src[c], bytes, cudaMemcpyHostToDevice, w->st));
+            w->h2d += (int64_t)bytes;
             D->bits[c] = (const uint32_t*)w->bits[c].p;
         }
         CUDA_TRY(w->marg[c].ensure(sizeof(int) * 3 * (size_t)d->num_snps));
@@ -197,6 +226,7 @@ episdet_status stage_dataset(Workspace* w, const episdet_dataset* d, bool valida
     if (validate) {
         int bad = 0;
         CUDA_TRY(cudaMemcpyAsync(&bad, w->flag.p, sizeof(int), cudaMemcpyDeviceToHost, w->st));
+        w->d2h += sizeof(int);
         CUDA_TRY(cudaStreamSynchronize(w->st));
         if (bad)
             return set_error(EPISDET_ERR_INVALID_INPUT,
@@ -243,9 +273,12 @@ static episdet_status run_simt(Workspace* w, const DevData& D0, const ScoreTable
         CUDA_TRY(cudaMemcpyAsync(w->tiles.p, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice, w->st));
         if (progress)
             for (int i = 0; i < bs_lines; ++i) printf("Outer loop iteration %d out of %d\n", i, bs_lines);
+        w->h2d += (int64_t)(sizeof(int2) * tiles.size());
+        CUDA_TRY(timer_begin(w));
         search2_simt_kernel<<<grid, kSimtBlockThreads, kSimtSmem2, w->st>>>(
             D, T, (const int2*)w->tiles.p, (int)tiles.size(), fb, fe, *S, 0, nullptr, nullptr);
         CHECK_LAUNCH();
+        CUDA_TRY(timer_end(w));
         ++*launches;
         return EPISDET_OK;
     }
@@ -275,8 +308,10 @@ static episdet_status run_simt(Workspace* w, const DevData& D0, const ScoreTable
         if (progress && x % 256 == 0) printf("Outer loop iteration %d out of %d\n", x / 256, bs_lines);
         int ty0 = (x + 1) / kSimtTileSnps;
         int n3 = off[nt] - off[ty0];
+        CUDA_TRY(timer_begin(w));
         search3_simt_kernel<<<grid, kSimtBlockThreads, kSimtSmem3, w->st>>>(D, T, x, d_tiles3 + off[ty0], n3, *S);
         CHECK_LAUNCH();
+        CUDA_TRY(timer_end(w));
         ++*launches;
     }
     return EPISDET_OK;
@@ -305,6 +340,7 @@ static episdet_status finish(Workspace* w, const DevData& D, const ScoreTables& 
     CUDA_TRY(cudaMemcpyAsync(&dev_err, w->tensor_flag.p, sizeof(int), cudaMemcpyDeviceToHost, w->st));
     CUDA_TRY(cudaEventRecord(w->e1, w->st));
     CUDA_TRY(cudaStreamSynchronize(w->st));
+    w->d2h += (int64_t)(sizeof(Cand) + sizeof(double)) * k + 2 * sizeof(int);
     if (dev_err)
         return set_error(EPISDET_ERR_TIMEOUT, "a bounded device wait gave up (code %d); results discarded", dev_err);
     if (cnt < 1) return set_error(EPISDET_ERR_INTERNAL, "no candidate survived the search");
@@ -399,6 +435,7 @@ episdet_status search_locked(Workspace* w, const episdet_dataset* data, const ep
                              episdet_result* result) {
     auto t0 = std::chrono::steady_clock::now();
     CUDA_TRY(cudaSetDevice(o.device));
+    begin_call(w, o);
     uint32_t* keep_snps = result->top_snps;
     float* keep32 = result->top_fp32;
     double* keep64 = result->top_fp64;
@@ -420,10 +457,10 @@ episdet_status search_locked(Workspace* w, const episdet_dataset* data, const ep
     CUDA_TRY(cudaEventRecord(w->e0, w->st));
     Slots S;
     bool progress = (o.flags & EPISDET_FLAG_PROGRESS) != 0;
-    if (o.engine == EPISDET_ENGINE_TENSOR)
-        st = run_tensor(w, D, T, o, fb, fe, &S, &launches, progress);
-    else
+    if (o.engine == EPISDET_ENGINE_SIMT)
         st = run_simt(w, D, T, o, fb, fe, &S, &launches, progress);
+    else
+        st = run_tensor(w, D, T, o, fb, fe, &S, &launches, progress);
     if (st != EPISDET_OK) return st;
     st = finish(w, D, T, o, S, result, &launches);
     if (st != EPISDET_OK) return st;
@@ -433,6 +470,19 @@ episdet_status search_locked(Workspace* w, const episdet_dataset* data, const ep
     result->sets_evaluated = sets_in_slab(o.order, data->num_snps, fb, fe);
     result->rounds = reference_rounds(o.order, data->num_snps);
     result->kernel_launches = launches;
+    result->count_kernel_launches = w->count_launches;
+    result->executed_macs = w->executed_macs;
+    result->h2d_bytes = w->h2d;
+    result->d2h_bytes = w->d2h;
+    if (w->timing) {
+        double sum = 0.0;
+        for (int i = 0; i + 1 < w->tev_used; i += 2) {
+            float t = 0.0f;
+            CUDA_TRY(cudaEventElapsedTime(&t, w->tev[i], w->tev[i + 1]));
+            sum += t;
+        }
+        result->count_kernel_ms = sum;
+    }
     result->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return EPISDET_OK;
 }

@@ -5,6 +5,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <mutex>
+#include <vector>
 
 #include "common.cuh"
 #include "device_data.cuh"
@@ -40,22 +41,31 @@ struct DevBuf {
 struct Workspace {
     int device = 0;
     int sms = 0;
-    cudaStream_t st = nullptr;
+    cudaStream_t st = nullptr;      // stream of the current call (own_st or the caller's)
+    cudaStream_t own_st = nullptr;  // the library's own stream
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     std::mutex mu;
     DevBuf bits[2], marg[2], pair4[2], t32, t64, slots, counts, tiles, merged, mcount, fp64, flag;
     DevBuf planes8;       // unpacked 0/1 byte operand rows (tensor engine)
-    DevBuf xsub[2];       // per-X sample-compacted operand rows (tensor engine, double buffered)
+    DevBuf xsub[8];       // per-X sample-regrouped operand rows (tensor engine)
     DevBuf xinfo;         // per-X segment tables (tensor engine)
     DevBuf tensor_flag;   // device error / progress words of the tensor engine
     DevBuf perm_planes, perm_cls[2], perm_idx;  // phenotype-permutation staging
+    // Per-call accounting.
+    int64_t h2d = 0, d2h = 0;
+    bool timing = false;
+    std::vector<cudaEvent_t> tev;  // event pool: (start, end) around each counting launch
+    int tev_used = 0;
+    int64_t count_launches = 0;
+    double executed_macs = 0.0;
     int tab_score = -1, tab_nc = -1, tab_nn = -1;
     float inv32 = 0.0f, hy32 = 0.0f;
     double inv64 = 0.0, hy64 = 0.0;
 
     void release_all() {
         DevBuf* all[] = {&bits[0], &bits[1], &marg[0], &marg[1], &pair4[0], &pair4[1], &t32, &t64, &slots,
-                         &counts, &tiles, &merged, &mcount, &fp64, &flag, &planes8, &xsub[0], &xsub[1], &xinfo,
+                         &counts, &tiles, &merged, &mcount, &fp64, &flag, &planes8, &xsub[0], &xsub[1], &xsub[2], &xsub[3], &xsub[4], &xsub[5],
+                         &xsub[6], &xsub[7], &xinfo,
                          &tensor_flag, &perm_planes, &perm_cls[0], &perm_cls[1], &perm_idx};
         for (DevBuf* b : all) b->release();
         tab_score = tab_nc = tab_nn = -1;
@@ -68,6 +78,13 @@ episdet_status stage_dataset(Workspace* w, const episdet_dataset* d, bool valida
 episdet_status prepare_slots(Workspace* w, int nslots, int k, Slots* S);
 episdet_status check_options(const episdet_options* in, int M, episdet_options* o);
 episdet_status check_dataset(const episdet_dataset* d, int order);
+
+// Brackets one counting-kernel launch with events when timing is on.
+cudaError_t timer_begin(Workspace* w);
+cudaError_t timer_end(Workspace* w);
+
+// Selects the stream of this call and resets the per-call accounting.
+void begin_call(Workspace* w, const episdet_options& o);
 
 // One search; the caller holds w->mu and has validated the options.
 episdet_status search_locked(Workspace* w, const episdet_dataset* data, const episdet_options& o,

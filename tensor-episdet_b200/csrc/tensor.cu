@@ -68,15 +68,30 @@ struct XInfo {
     Seg seg[4];     // [class*2 + kept genotype]
 };
 
+constexpr int kMaxGroup = 4;  // first SNPs (X) per triplet launch
+constexpr int kBand = 12;     // tile-band edge of the triplet tile order
+
+// One tensor map per X of a launch (each X has its own regrouped operand rows).
+struct TmapPack {
+    CUtensorMap m[kMaxGroup];
+};
+
+// Tiles [cum, next cum) of a launch belong to group member g: X = x, list tiles.
+struct GroupDesc {
+    const int2* tiles;  // (A tile, B tile) in 64-SNP units
+    int cum;
+    int x;
+    const XInfo* xinfo;
+};
+
 struct TcParams {
     DevData D;
     ScoreTables T;
     Slots S;
-    const int2* tiles;  // (A tile, B tile) in 64-SNP units
-    int ntiles;
+    int ngroup;
+    int ntiles;  // total over the group
+    GroupDesc grp[kMaxGroup];
     int mode;
-    int xsnp;
-    const XInfo* xinfo;
     Seg seg2[2];
     int first_begin, first_end;
     uint4* pair_out0;
@@ -87,7 +102,23 @@ struct TcParams {
 constexpr size_t kSmemTopk = (size_t)kStages * kStageBytes;
 constexpr size_t kSmemBars = kSmemTopk + (size_t)kCap * sizeof(Cand);
 constexpr size_t kSmemMisc = kSmemBars + 16 * sizeof(uint64_t);
-constexpr size_t kSmemTotal = kSmemMisc + 64 + 1024;
+constexpr size_t kSmemGroup = kSmemMisc + 64;
+constexpr size_t kSmemTotal = kSmemGroup + 256 + 1024;
+
+// Per-launch copy of each group member's segments in shared memory.
+struct GroupSm {
+    Seg seg[4];
+    int ga, gb, x, empty_mask;
+};
+static_assert(sizeof(GroupSm) * kMaxGroup <= 256, "group table size");
+
+__device__ __forceinline__ int group_of(const TcParams& P, int t) {
+    int g = 0;
+#pragma unroll
+    for (int i = 1; i < kMaxGroup; ++i)
+        if (i < P.ngroup && t >= P.grp[i].cum) g = i;
+    return g;
+}
 
 // ------------------------------------------------------------ operand prep
 // Packed planes -> 0/1 bytes.  Row r = 2*snp + g holds the cases' bytes in
@@ -204,36 +235,87 @@ __global__ void __launch_bounds__(1024) xinfo_kernel(DevData D, int X, XInfo* in
 // Regrouped operand rows for one X: row r, class c, segment s holds byte
 // bit(r, idx[c][s][k]) at column seg.kb0*128 + k (zero past the segment's
 // length up to its 128-byte end).  Rows below row0 are not needed by X.
-__global__ void __launch_bounds__(256) compact_kernel(DevData D, const XInfo* __restrict__ info,
-                                                      const int* __restrict__ idx, int max_n, int row0, int rows,
-                                                      uint8_t* __restrict__ out, int pitch) {
-    const int cmax0 = (D.W[0] * 32 + 256) / 16, cmax1 = (D.W[1] * 32 + 256) / 16;
-    const int chunks = cmax0 + cmax1;
-    const long total = (long)rows * chunks;
-    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
-        int r = row0 + (int)(t / chunks);
-        int ch = (int)(t % chunks);
-        int c = ch < cmax0 ? 0 : 1;
-        int k = (ch - (c ? cmax0 : 0)) * 16;
-        int la = info->len[c][0], lb = info->len[c][1];
-        int pa = ((la + kKB - 1) / kKB) * kKB, pb = ((lb + kKB - 1) / kKB) * kKB;
-        if (k >= pa + pb) continue;
-        int s = k < pa ? 0 : 1;
-        int kk = k - (s ? pa : 0);
-        int len = s ? lb : la;
-        const int* ix = idx + ((size_t)c * 2 + s) * max_n;
-        const uint32_t* src = D.bits[c] + (size_t)r * D.W[c];
+//
+// Output-stationary: a CTA owns 4096 output bytes of one class region (the two
+// segments back to back) for kCmpRows rows.  Each thread keeps the source
+// sample indices of its 16 output bytes in registers and reuses them for every
+// row; the source words those samples fall in are staged in shared memory per
+// row when their span fits.  Sized (<= 64 registers, ~21 KB shared memory) so
+// that one CTA fits on an SM beside a tc_kernel CTA.
+constexpr int kCmpOut = 4096;
+constexpr int kCmpThreads = 256;
+constexpr int kCmpRows = 16;
+constexpr int kCmpSpanWords = 5120;
+
+__host__ __device__ inline int cmp_chunks(int words) { return (words * 32 + 256 + kCmpOut - 1) / kCmpOut; }
+
+__global__ void __launch_bounds__(kCmpThreads, 4)
+    compact_kernel(DevData D, const XInfo* __restrict__ info, const int* __restrict__ idx, int max_n, int row0,
+                   int nrows, uint8_t* __restrict__ out, int pitch) {
+    __shared__ uint32_t s_src[kCmpSpanWords];
+    __shared__ int s_lo, s_hi;
+    const int C0 = cmp_chunks(D.W[0]);
+    const int c = (int)blockIdx.x < C0 ? 0 : 1;
+    const int chunk = (int)blockIdx.x - (c ? C0 : 0);
+    const int la = info->len[c][0], lb = info->len[c][1];
+    const int pa = ((la + kKB - 1) / kKB) * kKB, pb = ((lb + kKB - 1) / kKB) * kKB;
+    const int region = pa + pb;
+    const int k0 = chunk * kCmpOut;
+    if (k0 >= region) return;  // uniform over the CTA
+    const int kk0 = k0 + 16 * (int)threadIdx.x;
+    const int* ia = idx + ((size_t)c * 2 + 0) * max_n;
+    const int* ib = idx + ((size_t)c * 2 + 1) * max_n;
+    int src[16];
+    int lo = 0x7FFFFFFF, hi = -1;
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+        const int k = kk0 + e;
+        int s = -1;
+        if (k < pa) {
+            if (k < la) s = __ldg(ia + k);
+        } else if (k < region) {
+            if (k - pa < lb) s = __ldg(ib + (k - pa));
+        }
+        src[e] = s;
+        if (s >= 0) {
+            lo = min(lo, s >> 5);
+            hi = max(hi, s >> 5);
+        }
+    }
+    if (threadIdx.x == 0) {
+        s_lo = 0x7FFFFFFF;
+        s_hi = -1;
+    }
+    __syncthreads();
+    if (hi >= 0) {
+        atomicMin(&s_lo, lo);
+        atomicMax(&s_hi, hi);
+    }
+    __syncthreads();
+    const int wlo = s_lo, whi = s_hi;
+    const bool staged = whi >= wlo && whi - wlo + 1 <= kCmpSpanWords;
+    const int W = D.W[c];
+    const int colbase = (c ? D.W[0] * 32 + 256 : 0) + kk0;
+    const int rbeg = row0 + (int)blockIdx.y * kCmpRows;
+    const int rend = min(row0 + nrows, rbeg + kCmpRows);
+    for (int row = rbeg; row < rend; ++row) {
+        const uint32_t* srow = D.bits[c] + (size_t)row * W;
+        if (staged) {
+            for (int w = wlo + (int)threadIdx.x; w <= whi; w += kCmpThreads) s_src[w - wlo] = __ldg(srow + w);
+            __syncthreads();
+        }
         uint32_t o[4] = {0, 0, 0, 0};
 #pragma unroll
         for (int e = 0; e < 16; ++e) {
-            if (kk + e < len) {
-                int j = __ldg(ix + kk + e);
-                uint32_t bit = (__ldg(src + (j >> 5)) >> (31 - (j & 31))) & 1u;
-                o[e >> 2] |= bit << (8 * (e & 3));
+            const int s = src[e];
+            if (s >= 0) {
+                const uint32_t word = staged ? s_src[(s >> 5) - wlo] : __ldg(srow + (s >> 5));
+                o[e >> 2] |= ((word >> (31 - (s & 31))) & 1u) << (8 * (e & 3));
             }
         }
-        int col = info->seg[c * 2 + s].kb0 * kKB + kk;
-        *reinterpret_cast<uint4*>(out + (size_t)r * pitch + col) = make_uint4(o[0], o[1], o[2], o[3]);
+        if (kk0 < region)
+            *reinterpret_cast<uint4*>(out + (size_t)row * pitch + colbase) = make_uint4(o[0], o[1], o[2], o[3]);
+        if (staged) __syncthreads();
     }
 }
 
@@ -241,7 +323,7 @@ __device__ __forceinline__ void record_error(int* err, int code) { atomicCAS(err
 
 // ------------------------------------------------------------------ kernel
 __global__ void __launch_bounds__(kThreads, 1)
-    tc_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ TcParams P) {
+    tc_kernel(const __grid_constant__ TmapPack tm, const __grid_constant__ TcParams P) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* stages = smem;
@@ -261,22 +343,30 @@ __global__ void __launch_bounds__(kThreads, 1)
     volatile int* abort = s_abort;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    GroupSm* s_grp = reinterpret_cast<GroupSm*>(smem + kSmemGroup);
     const int mode = P.mode;
-    int nseg = 2;
-    Seg seg[4];
-    int ga = 0, gb = 1;
-    if (mode == kTriplets) {
-        nseg = 4;
-#pragma unroll
-        for (int s = 0; s < 4; ++s) seg[s] = P.xinfo->seg[s];
-        ga = P.xinfo->ga;
-        gb = P.xinfo->gb;
-    } else {
-        seg[0] = P.seg2[0];
-        seg[1] = P.seg2[1];
-        seg[2] = seg[3] = Seg{0, 0};
-    }
+    const int nseg = mode == kTriplets ? 4 : 2;
     const int nbuf = 4 / nseg;
+    if (threadIdx.x < P.ngroup) {
+        GroupSm gs;
+        if (mode == kTriplets) {
+            const XInfo* xi = P.grp[threadIdx.x].xinfo;
+            for (int s = 0; s < 4; ++s) gs.seg[s] = xi->seg[s];
+            gs.ga = xi->ga;
+            gs.gb = xi->gb;
+        } else {
+            gs.seg[0] = P.seg2[0];
+            gs.seg[1] = P.seg2[1];
+            gs.seg[2] = gs.seg[3] = Seg{0, 0};
+            gs.ga = 0;
+            gs.gb = 1;
+        }
+        gs.x = P.grp[threadIdx.x].x;
+        gs.empty_mask = 0;
+        for (int s = 0; s < 4; ++s)
+            if (gs.seg[s].kb1 <= gs.seg[s].kb0) gs.empty_mask |= 1 << s;
+        s_grp[threadIdx.x] = gs;
+    }
 
     if (threadIdx.x == 0) {
         for (int i = 0; i < kStages; ++i) {
@@ -297,7 +387,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         ptx::tmem_alloc(s_tmem, 512);
         ptx::tmem_relinquish();
     }
-    if (warp == 0 && lane == 0) ptx::prefetch_tmap(&tmap);
+    if (warp == 0 && lane < P.ngroup) ptx::prefetch_tmap(&tm.m[lane]);
     ptx::tc_fence_before();
     __syncthreads();
     ptx::tc_fence_after();
@@ -316,7 +406,10 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
             bool ok = true;
             for (int t = blockIdx.x; ok && t < P.ntiles; t += gridDim.x) {
-                const int2 tl = P.tiles[t];
+                const int g = group_of(P, t);
+                const int2 tl = P.grp[g].tiles[t - P.grp[g].cum];
+                const Seg* seg = s_grp[g].seg;
+                const CUtensorMap* tmap = &tm.m[g];
                 for (int s = 0; ok && s < nseg; ++s)
                     for (int kb = seg[s].kb0; kb < seg[s].kb1; ++kb) {
                         if (!ptx::mbar_wait(&empty[stage], phase ^ 1, abort, kWaitLimitNs)) {
@@ -325,8 +418,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                         }
                         ptx::mbar_arrive_expect_tx(&full[stage], kStageBytes);
                         uint8_t* sa = stages + (size_t)stage * kStageBytes;
-                        ptx::tma_load_2d(sa, &tmap, kb * kKB, tl.x * kTileRows, &full[stage]);
-                        ptx::tma_load_2d(sa + kTileBytes, &tmap, kb * kKB, tl.y * kTileRows, &full[stage]);
+                        ptx::tma_load_2d(sa, tmap, kb * kKB, tl.x * kTileRows, &full[stage]);
+                        ptx::tma_load_2d(sa + kTileBytes, tmap, kb * kKB, tl.y * kTileRows, &full[stage]);
                         pend[stage] = true;
                         pend_phase[stage] = phase;
                         if (++stage == kStages) {
@@ -351,6 +444,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             bool ok = true;
             int local = 0;
             for (int t = blockIdx.x; ok && t < P.ntiles; t += gridDim.x, ++local) {
+                const Seg* seg = s_grp[group_of(P, t)].seg;
                 const int b = local % nbuf;
                 const uint32_t use = (uint32_t)(local / nbuf);
                 if (!ptx::mbar_wait(&tempty[b], (use & 1) ^ 1, abort, kWaitLimitNs)) {
@@ -401,9 +495,6 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int M = P.D.M;
         LocalTopK<kCap, kEpiThreads> tk{tbuf, s_count, s_thr, P.S.k, etid};
         if (mode != kPairsStore) tk.load(P.S.lists + (size_t)blockIdx.x * P.S.k, P.S.counts[blockIdx.x], bar);
-        bool seg_empty[4];
-#pragma unroll
-        for (int s = 0; s < 4; ++s) seg_empty[s] = seg[s].kb1 <= seg[s].kb0;
         bool ok = true;
         int local = 0;
         for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x, ++local) {
@@ -419,13 +510,15 @@ __global__ void __launch_bounds__(kThreads, 1)
                 break;
             }
             ptx::tc_fence_after();
-            const int2 tl = P.tiles[t];
+            const int g = group_of(P, t);
+            const int2 tl = P.grp[g].tiles[t - P.grp[g].cum];
+            const int ga = s_grp[g].ga, gb = s_grp[g].gb, emask = s_grp[g].empty_mask;
             const int arow = tl.x * kTileSnps + yl;  // this thread's A SNP (pairs: a, triplets: Y)
             const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * nseg * 128);
             // Per-row constants.
             int ma[2][3] = {{0, 0, 0}, {0, 0, 0}}, mx[2][3] = {{0, 0, 0}, {0, 0, 0}};
             int xy9[2][9];
-            const int X = P.xsnp;
+            const int X = s_grp[g].x;
             const bool row_ok = arow < M && (mode != kTriplets || arow > X);
             if (row_ok) {
 #pragma unroll
@@ -451,7 +544,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 }
 #pragma unroll
                 for (int s = 0; s < 4; ++s)
-                    if (s >= nseg || seg_empty[s])
+                    if (s >= nseg || ((emask >> s) & 1))
 #pragma unroll
                         for (int e = 0; e < 16; ++e) v[s][e] = 0;
                 // Partner lane (other plane of the same A SNP) sends the counts of our 4 B SNPs.
@@ -612,8 +705,9 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     unpack_kernel<<<grid_for((long)rows * (pitch2 / 16), 256), 256, 0, w->st>>>(D, P2, rows, pitch2);
     CHECK_LAUNCH();
     ++*launches;
-    CUtensorMap tm2;
-    st = make_tmap(&tm2, P2, (uint64_t)rows, (uint64_t)pitch2);
+    TmapPack tm2;
+    memset(&tm2, 0, sizeof(tm2));
+    st = make_tmap(&tm2.m[0], P2, (uint64_t)rows, (uint64_t)pitch2);
     if (st != EPISDET_OK) return st;
 
     const int nt = (M + kTileSnps - 1) / kTileSnps;
@@ -637,12 +731,17 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
         CUDA_TRY(cudaMemcpyAsync(w->tiles.p, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice, w->st));
         if (progress)
             for (int i = 0; i < bs_lines; ++i) printf("Outer loop iteration %d out of %d\n", i, bs_lines);
-        p.tiles = (const int2*)w->tiles.p;
+        w->h2d += (int64_t)(sizeof(int2) * tiles.size());
+        p.ngroup = 1;
+        p.grp[0] = GroupDesc{(const int2*)w->tiles.p, 0, -1, nullptr};
         p.ntiles = (int)tiles.size();
         p.mode = kPairsScore;
+        CUDA_TRY(timer_begin(w));
         tc_kernel<<<grid, kThreads, kSmemTotal, w->st>>>(tm2, p);
         CHECK_LAUNCH();
+        CUDA_TRY(timer_end(w));
         ++*launches;
+        if (w->timing) w->executed_macs = (double)tiles.size() * kTileRows * kTileRows * (double)pitch2;
         return EPISDET_OK;
     }
 
@@ -652,17 +751,32 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
         D.pair4[c] = (const uint4*)w->pair4[c].p;
     }
     p.D = D;
-    std::vector<int2> ptiles, all3;
+    std::vector<int2> ptiles;
     for (int a = fb / kTileSnps; a < nt; ++a)
         for (int b = a; b < nt; ++b) ptiles.push_back(make_int2(a, b));
-    for (int a = 0; a < nt; ++a)
-        for (int b = a; b < nt; ++b) all3.push_back(make_int2(a, b));
-    CUDA_TRY(w->tiles.ensure(sizeof(int2) * (ptiles.size() + all3.size())));
+    // Triplet tile lists, one per first row tile t0 = tile(X+1): every (A, B)
+    // tile pair with t0 <= A <= B, ordered in bands of kBand x kBand tiles so
+    // that a wave of concurrent tiles shares few A and B row panels in L2.
+    const int t_first = (fb + 1) / kTileSnps;
+    std::vector<int2> lists;
+    std::vector<size_t> list_off((size_t)nt + 1, 0);
+    for (int t0 = t_first; t0 < nt; ++t0) {
+        list_off[t0] = lists.size();
+        const int T = nt - t0, nb = (T + kBand - 1) / kBand;
+        for (int ba = 0; ba < nb; ++ba)
+            for (int bb = ba; bb < nb; ++bb)
+                for (int a = ba * kBand; a < std::min(T, (ba + 1) * kBand); ++a)
+                    for (int b = std::max(a, bb * kBand); b < std::min(T, (bb + 1) * kBand); ++b)
+                        lists.push_back(make_int2(t0 + a, t0 + b));
+    }
+    CUDA_TRY(w->tiles.ensure(sizeof(int2) * (ptiles.size() + lists.size())));
     int2* d_ptiles = (int2*)w->tiles.p;
-    int2* d_all3 = d_ptiles + ptiles.size();
+    int2* d_lists = d_ptiles + ptiles.size();
     CUDA_TRY(cudaMemcpyAsync(d_ptiles, ptiles.data(), sizeof(int2) * ptiles.size(), cudaMemcpyHostToDevice, w->st));
-    CUDA_TRY(cudaMemcpyAsync(d_all3, all3.data(), sizeof(int2) * all3.size(), cudaMemcpyHostToDevice, w->st));
-    p.tiles = d_ptiles;
+    CUDA_TRY(cudaMemcpyAsync(d_lists, lists.data(), sizeof(int2) * lists.size(), cudaMemcpyHostToDevice, w->st));
+    w->h2d += (int64_t)(sizeof(int2) * (ptiles.size() + lists.size()));
+    p.ngroup = 1;
+    p.grp[0] = GroupDesc{d_ptiles, 0, -1, nullptr};
     p.ntiles = (int)ptiles.size();
     p.mode = kPairsStore;
     p.pair_out0 = (uint4*)w->pair4[0].p;
@@ -671,18 +785,19 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     CHECK_LAUNCH();
     ++*launches;
 
-    // Per-X regrouped operands (double buffered) and their segment tables.
+    // Regrouped operands of the kMaxGroup X values of a launch, and their segment tables.
     const int pitchx = Kc + 256 + Kn + 256;
     const int max_n = std::max(D.n[0], D.n[1]);
-    for (int i = 0; i < 2; ++i) CUDA_TRY(w->xsub[i].ensure((size_t)rows * pitchx));
+    for (int i = 0; i < kMaxGroup; ++i) CUDA_TRY(w->xsub[i].ensure((size_t)rows * pitchx));
     const size_t info_bytes = 256;
     const size_t idx_bytes = sizeof(int) * 4 * (size_t)max_n;
-    CUDA_TRY(w->xinfo.ensure(2 * (info_bytes + idx_bytes)));
-    CUtensorMap tmx[2];
-    XInfo* d_info[2];
-    int* d_idx[2];
-    for (int i = 0; i < 2; ++i) {
-        st = make_tmap(&tmx[i], w->xsub[i].p, (uint64_t)rows, (uint64_t)pitchx);
+    CUDA_TRY(w->xinfo.ensure(kMaxGroup * (info_bytes + idx_bytes)));
+    TmapPack tmx;
+    memset(&tmx, 0, sizeof(tmx));
+    XInfo* d_info[kMaxGroup];
+    int* d_idx[kMaxGroup];
+    for (int i = 0; i < kMaxGroup; ++i) {
+        st = make_tmap(&tmx.m[i], w->xsub[i].p, (uint64_t)rows, (uint64_t)pitchx);
         if (st != EPISDET_OK) return st;
         d_info[i] = (XInfo*)((uint8_t*)w->xinfo.p + i * (info_bytes + idx_bytes));
         d_idx[i] = (int*)((uint8_t*)d_info[i] + info_bytes);
@@ -691,25 +806,58 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     for (int t = 0; t < nt; ++t) off[t + 1] = off[t] + (nt - t);
     const int xend = std::min(fe, M - 2);
     p.mode = kTriplets;
-    for (int x = fb; x < xend; ++x) {
-        if (progress && x % 256 == 0) printf("Outer loop iteration %d out of %d\n", x / 256, bs_lines);
-        const int bi = x & 1;
-        const int t0 = (x + 1) / kTileSnps;
-        xinfo_kernel<<<2, 1024, 0, w->st>>>(D, x, d_info[bi], d_idx[bi], max_n);
+    for (int x0 = fb; x0 < xend; x0 += kMaxGroup) {
+        const int gn = std::min(kMaxGroup, xend - x0);
+        int cum = 0;
+        for (int g = 0; g < gn; ++g) {
+            const int x = x0 + g;
+            if (progress && x % 256 == 0) printf("Outer loop iteration %d out of %d\n", x / 256, bs_lines);
+            const int t0 = (x + 1) / kTileSnps;
+            xinfo_kernel<<<2, 1024, 0, w->st>>>(D, x, d_info[g], d_idx[g], max_n);
+            CHECK_LAUNCH();
+            const int row0 = 2 * t0 * kTileSnps;
+            const int nrows = rows - row0;
+            const dim3 cgrid(cmp_chunks(D.W[0]) + cmp_chunks(D.W[1]), (nrows + kCmpRows - 1) / kCmpRows);
+            compact_kernel<<<cgrid, kCmpThreads, 0, w->st>>>(D, d_info[g], d_idx[g], max_n, row0, nrows,
+                                                              (uint8_t*)w->xsub[g].p, pitchx);
+            CHECK_LAUNCH();
+            p.grp[g] = GroupDesc{d_lists + list_off[t0], cum, x, d_info[g]};
+            cum += off[nt] - off[t0];
+            *launches += 2;
+        }
+        p.ngroup = gn;
+        p.ntiles = cum;
+        CUDA_TRY(timer_begin(w));
+        tc_kernel<<<grid, kThreads, kSmemTotal, w->st>>>(tmx, p);
         CHECK_LAUNCH();
-        const int row0 = 2 * t0 * kTileSnps;
-        const int nrows = rows - row0;
-        const long cwork = (long)nrows * ((Kc + 256) / 16 + (Kn + 256) / 16);
-        compact_kernel<<<grid_for(cwork, 256), 256, 0, w->st>>>(D, d_info[bi], d_idx[bi], max_n, row0, nrows,
-                                                                 (uint8_t*)w->xsub[bi].p, pitchx);
-        CHECK_LAUNCH();
-        p.xsnp = x;
-        p.xinfo = d_info[bi];
-        p.tiles = d_all3 + off[t0];
-        p.ntiles = off[nt] - off[t0];
-        tc_kernel<<<grid, kThreads, kSmemTotal, w->st>>>(tmx[bi], p);
-        CHECK_LAUNCH();
-        *launches += 3;
+        CUDA_TRY(timer_end(w));
+        *launches += 1;
+    }
+    if (w->timing) {
+        // Tensor MACs issued: per X, tiles x 128 x 128 x the regrouped K extent,
+        // which follows from X's genotype counts exactly as xinfo_kernel derives it.
+        std::vector<int> mg[2];
+        for (int c = 0; c < 2; ++c) {
+            mg[c].resize((size_t)3 * M);
+            CUDA_TRY(cudaMemcpyAsync(mg[c].data(), D.marg[c], sizeof(int) * 3 * M, cudaMemcpyDeviceToHost, w->st));
+        }
+        CUDA_TRY(cudaStreamSynchronize(w->st));
+        w->d2h += (int64_t)(2 * sizeof(int) * 3 * M);
+        double macs = 0.0;
+        for (int x = fb; x < xend; ++x) {
+            int tot[3];
+            for (int g = 0; g < 3; ++g) tot[g] = mg[0][(size_t)g * M + x] + mg[1][(size_t)g * M + x];
+            int gd = 0;
+            if (tot[1] > tot[gd]) gd = 1;
+            if (tot[2] > tot[gd]) gd = 2;
+            long kext = 0;
+            for (int c = 0; c < 2; ++c)
+                for (int g = 0; g < 3; ++g)
+                    if (g != gd) kext += ((mg[c][(size_t)g * M + x] + kKB - 1) / kKB) * (long)kKB;
+            const int t0 = (x + 1) / kTileSnps;
+            macs += (double)(off[nt] - off[t0]) * kTileRows * kTileRows * (double)kext;
+        }
+        w->executed_macs = macs;
     }
     return EPISDET_OK;
 }

@@ -22,7 +22,7 @@ LIB_PATH = os.path.join(HERE, "lib", "libepisdet.so")
 SCORE_K2, SCORE_MI = 0, 1
 HOST, DEVICE = 0, 1
 ENGINE_AUTO, ENGINE_TENSOR, ENGINE_SIMT = 0, 1, 2
-FLAG_PROGRESS, FLAG_NO_VALIDATE = 0x1, 0x2
+FLAG_PROGRESS, FLAG_NO_VALIDATE, FLAG_TIMING = 0x1, 0x2, 0x4
 
 STATUS = {
     0: "EPISDET_OK",
@@ -66,14 +66,17 @@ class Cohort(ctypes.Structure):
 class Options(ctypes.Structure):
     _fields_ = [("order", ctypes.c_int32), ("score", ctypes.c_int32), ("top_k", ctypes.c_int32),
                 ("device", ctypes.c_int32), ("engine", ctypes.c_int32), ("first_begin", ctypes.c_int32),
-                ("first_end", ctypes.c_int32), ("flags", ctypes.c_uint32), ("reserved", ctypes.c_int32 * 8)]
+                ("first_end", ctypes.c_int32), ("flags", ctypes.c_uint32), ("stream", ctypes.c_uint64),
+                ("reserved", ctypes.c_int32 * 6)]
 
 
 class Result(ctypes.Structure):
     _fields_ = [("snps", ctypes.c_uint32 * 3), ("packed_indices", ctypes.c_uint64), ("score", ctypes.c_double),
                 ("score_fp32", ctypes.c_float), ("top_count", ctypes.c_int32), ("sets_evaluated", ctypes.c_int64),
                 ("rounds", ctypes.c_int64), ("seconds", ctypes.c_double), ("device_ms", ctypes.c_double),
-                ("kernel_launches", ctypes.c_uint64), ("top_capacity", ctypes.c_int32),
+                ("kernel_launches", ctypes.c_uint64), ("count_kernel_ms", ctypes.c_double),
+                ("count_kernel_launches", ctypes.c_int64), ("executed_macs", ctypes.c_double),
+                ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64), ("top_capacity", ctypes.c_int32),
                 ("top_snps", ctypes.POINTER(ctypes.c_uint32)), ("top_fp32", ctypes.POINTER(ctypes.c_float)),
                 ("top_fp64", ctypes.POINTER(ctypes.c_double))]
 
@@ -218,22 +221,29 @@ class SearchResult:
     seconds: float
     device_ms: float
     kernel_launches: int
+    count_kernel_ms: float
+    count_kernel_launches: int
+    executed_macs: float
+    h2d_bytes: int
+    d2h_bytes: int
     top_snps: np.ndarray = field(repr=False)
     top_fp32: np.ndarray = field(repr=False)
     top_fp64: np.ndarray = field(repr=False)
 
 
 def _ptr(a):
-    """(pointer, memory kind) of a numpy array or a CUDA tensor."""
-    if hasattr(a, "data_ptr") and getattr(a, "is_cuda", False):
-        return a.data_ptr(), DEVICE
+    """(pointer, memory kind) of a numpy array, a CUDA tensor or a (pinned) host tensor."""
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous() or a.element_size() != 4:
+            raise TypeError("tensors must be contiguous 32-bit")
+        return a.data_ptr(), (DEVICE if a.is_cuda else HOST)
     if not (isinstance(a, np.ndarray) and a.dtype == np.uint32 and a.flags["C_CONTIGUOUS"]):
         raise TypeError("planes must be C-contiguous uint32 numpy arrays or CUDA tensors")
     return a.ctypes.data, HOST
 
 
 def make_options(order=3, score="k2", top_k=1024, device=0, engine="auto", first_begin=0, first_end=0,
-                 flags=0) -> Options:
+                 flags=0, stream=0) -> Options:
     o = Options()
     lib().episdet_default_options(ctypes.byref(o))
     o.order = order
@@ -243,6 +253,7 @@ def make_options(order=3, score="k2", top_k=1024, device=0, engine="auto", first
     o.engine = {"auto": ENGINE_AUTO, "tensor": ENGINE_TENSOR, "simt": ENGINE_SIMT}[engine] \
         if isinstance(engine, str) else int(engine)
     o.first_begin, o.first_end, o.flags = first_begin, first_end, flags
+    o.stream = int(stream)
     return o
 
 
@@ -261,13 +272,15 @@ def _to_result(order: int, r: Result, bufs) -> SearchResult:
     return SearchResult(snps=tuple(int(v) for v in r.snps[:order]), score=r.score, score_fp32=r.score_fp32,
                         packed_indices=int(r.packed_indices), sets_evaluated=int(r.sets_evaluated),
                         rounds=int(r.rounds), seconds=r.seconds, device_ms=r.device_ms,
-                        kernel_launches=int(r.kernel_launches), top_snps=bufs[0][:n, :order].copy(),
+                        kernel_launches=int(r.kernel_launches), count_kernel_ms=r.count_kernel_ms,
+                        count_kernel_launches=int(r.count_kernel_launches), executed_macs=r.executed_macs,
+                        h2d_bytes=int(r.h2d_bytes), d2h_bytes=int(r.d2h_bytes), top_snps=bufs[0][:n, :order].copy(),
                         top_fp32=bufs[1][:n].copy(), top_fp64=bufs[2][:n].copy())
 
 
 def search(cases, controls, num_cases: int, num_controls: int, *, num_snps: Optional[int] = None, order: int = 3,
            score="k2", top_k: int = 1024, device: int = 0, engine="auto", first_begin: int = 0, first_end: int = 0,
-           flags: int = 0) -> SearchResult:
+           flags: int = 0, stream: int = 0) -> SearchResult:
     """Exhaustive search; cases/controls are host uint32 arrays or CUDA tensors in the plane format."""
     pc, mc = _ptr(cases)
     pn, mn = _ptr(controls)
@@ -275,7 +288,7 @@ def search(cases, controls, num_cases: int, num_controls: int, *, num_snps: Opti
         raise TypeError("cases and controls must live in the same memory")
     M = num_snps if num_snps is not None else int(cases.shape[0])
     d = Dataset(pc, pn, M, num_cases, num_controls, mc)
-    o = make_options(order, score, top_k, device, engine, first_begin, first_end, flags)
+    o = make_options(order, score, top_k, device, engine, first_begin, first_end, flags, stream)
     r, bufs = _result_buffers(top_k)
     _check(lib().episdet_search(ctypes.byref(d), ctypes.byref(o), ctypes.byref(r)))
     return _to_result(order, r, bufs)

@@ -1,0 +1,48 @@
+"""Runs one search on a seeded synthetic dataset and prints a JSON summary.
+
+  python tensor-episdet_b200/run_synthetic.py --snps 2048 --cases 65536 --controls 65536 \
+      --order 3 --score k2 [--first-begin 0 --first-end 1] [--engine tensor|simt] [--repeat 1]
+
+Useful to reproduce a workload, to time one configuration, or as the
+command of a profiler capture of a single counting launch (a one-SNP slab
+with --first-end 1 launches the triplet kernel once).
+"""
+import argparse
+import json
+import os
+import sys
+
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+
+import episdet  # noqa: E402
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--snps", type=int, default=1024)
+    ap.add_argument("--cases", type=int, default=8192)
+    ap.add_argument("--controls", type=int, default=8192)
+    ap.add_argument("--order", type=int, default=3)
+    ap.add_argument("--score", default="k2")
+    ap.add_argument("--engine", default="auto")
+    ap.add_argument("--first-begin", type=int, default=0)
+    ap.add_argument("--first-end", type=int, default=0)
+    ap.add_argument("--top-k", type=int, default=1024)
+    ap.add_argument("--seed", type=int, default=0xE917)
+    ap.add_argument("--maf", type=float, nargs=2, default=(0.05, 0.5))
+    ap.add_argument("--repeat", type=int, default=1)
+    a = ap.parse_args()
+    cases, controls = episdet.generate(a.seed, a.snps, a.cases, a.controls, maf=tuple(a.maf))
+    for i in range(a.repeat):
+        r = episdet.search(cases, controls, a.cases, a.controls, order=a.order, score=a.score, top_k=a.top_k,
+                           engine=a.engine, first_begin=a.first_begin, first_end=a.first_end,
+                           flags=episdet.FLAG_TIMING)
+    n = a.cases + a.controls
+    print(json.dumps({"snps": list(r.snps), "score": r.score, "sets": r.sets_evaluated, "device_ms": r.device_ms,
+                      "count_kernel_ms": r.count_kernel_ms, "count_launches": r.count_kernel_launches,
+                      "executed_macs": r.executed_macs, "launches": r.kernel_launches,
+                      "tera_sets_samples_per_s": r.sets_evaluated * n / (r.device_ms * 1e-3) / 1e12}))
+
+
+if __name__ == "__main__":
+    main()
