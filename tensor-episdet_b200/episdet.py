@@ -43,6 +43,7 @@ EXPORTED = [
     "episdet_search_perm", "episdet_read_dataset", "episdet_free_dataset", "episdet_write_dataset",
     "episdet_generate", "episdet_generate_cohort", "episdet_generate_labels", "episdet_n_choose_k",
     "episdet_status_string", "episdet_last_error", "episdet_abi_version", "episdet_release_workspace",
+    "episdet_search_pairs_noalloc",
 ]
 
 
@@ -131,6 +132,8 @@ def lib() -> ctypes.CDLL:
     L.episdet_abi_version.restype = ctypes.c_int32
     L.episdet_release_workspace.argtypes = [ctypes.c_int32]
     L.episdet_release_workspace.restype = ctypes.c_int
+    L.episdet_search_pairs_noalloc.argtypes = [P(Dataset), P(Options), P(Result)]
+    L.episdet_search_pairs_noalloc.restype = ctypes.c_int
     _lib = L
     return L
 
@@ -292,6 +295,22 @@ def search(cases, controls, num_cases: int, num_controls: int, *, num_snps: Opti
     r, bufs = _result_buffers(top_k)
     _check(lib().episdet_search(ctypes.byref(d), ctypes.byref(o), ctypes.byref(r)))
     return _to_result(order, r, bufs)
+
+
+def search_pairs_noalloc(cases, controls, num_cases: int, num_controls: int, *, num_snps: int, score="k2",
+                         top_k: int = 1024, device: int = 0, first_begin: int = 0, first_end: int = 0,
+                         stream: int = 0) -> SearchResult:
+    """Pairs search through the entry point that allocates no device memory
+    (for callers whose memory is owned by a pool or that cannot synchronise
+    for cudaFree).  cases/controls must be device-resident (CUDA tensors);
+    limits: 4096 SNPs, 131072 samples, top_k 1024."""
+    pc, mc = _ptr(cases)
+    pn, mn = _ptr(controls)
+    d = Dataset(pc, pn, num_snps, num_cases, num_controls, mc)
+    o = make_options(2, score, top_k, device, "simt", first_begin, first_end, 0, stream)
+    r, bufs = _result_buffers(top_k)
+    _check(lib().episdet_search_pairs_noalloc(ctypes.byref(d), ctypes.byref(o), ctypes.byref(r)))
+    return _to_result(2, r, bufs)
 
 
 def search_batched(cohorts, options) -> list:
