@@ -151,3 +151,20 @@ def test_fp32_error_is_small(oracle):
     r = oracle.search(cases, controls, nc, nn, order=3, score="k2", top_k=35)
     rel = np.abs(r["top_fp32"].astype(np.float64) - r["top_fp64"]) / np.abs(r["top_fp64"])
     assert rel.max() < 1e-5
+
+
+@pytest.mark.parametrize("score", ["k2", "mi"])
+def test_fp32_error_with_large_counts(oracle, score):
+    """Cells holding thousands of samples (table values near 1e5 for K2): the
+    FP32 ranking score stays within 1e-5 of the exact FP64 score and the
+    reported optimum is the FP64 optimum of the candidate list."""
+    rng = np.random.default_rng(11)
+    M, nc, nn = 10, 9000, 11000
+    g = rng.integers(0, 3, size=(M, nc + nn)).astype(np.int8)
+    g[:, : (nc + nn) // 2] = 0  # large cells: many counts well above 8192
+    cases, controls = oracle.pack(g[:, :nc]), oracle.pack(g[:, nc:])
+    r = oracle.search(cases, controls, nc, nn, order=2, score=score, top_k=math.comb(M, 2))
+    rel = np.abs(r["top_fp32"].astype(np.float64) - r["top_fp64"]) / np.abs(r["top_fp64"])
+    assert rel.max() < 1e-5
+    best = min(range(len(r["top"])), key=lambda i: (r["top_fp64"][i] * (1 if score == "k2" else -1), r["top"][i]))
+    assert tuple(r["best"]) == tuple(r["top"][best])

@@ -42,7 +42,8 @@ def test_known_answers(episdet, oracle, c, score, engine):
 
 @pytest.mark.parametrize("engine", ENGINES)
 @pytest.mark.parametrize("order,M,nc,nn", [(2, 200, 3000, 2500), (3, 60, 700, 1300), (2, 70, 1, 4097),
-                                           (3, 40, 31, 1025), (3, 45, 4097, 33), (2, 129, 1023, 1024)])
+                                           (3, 40, 31, 1025), (3, 45, 4097, 33), (2, 129, 1023, 1024),
+                                           (2, 100, 9000, 11000), (3, 40, 12000, 9000)])
 @pytest.mark.parametrize("score", ["k2", "mi"])
 def test_random_datasets(episdet, oracle, order, M, nc, nn, score, engine):
     cases, controls = episdet.generate(100 + M + nc, M, nc, nn)
