@@ -49,9 +49,13 @@ constexpr int kStages = 4;
 constexpr int kTileBytes = kTileRows * kKB;
 constexpr int kStageBytes = 2 * kTileBytes;
 constexpr int kCap = 4096;
-constexpr int kThreads = 192;
-constexpr int kEpiThreads = 128;
-constexpr int kEpiPerStep = kEpiThreads * 4;
+// Warp 0 issues TMA, warp 1 MMAs; warps 2..9 are the epilogue, two per TMEM
+// lane quarter (warp % 4), each taking half of the 128 accumulator columns in
+// chunks of 8 columns (4 B SNPs x 2 planes; each lane scores 2 of the 4).
+constexpr int kThreads = 320;
+constexpr int kEpiThreads = 256;
+constexpr int kEpiPerStep = kEpiThreads * 2;
+static_assert(kMaxTopK + kEpiPerStep <= 4096, "candidate buffer too small for one step of offers");
 constexpr uint64_t kWaitLimitNs = 4000000000ull;
 constexpr uint32_t kIdesc = ptx::idesc_u8(128);
 
@@ -487,9 +491,10 @@ __global__ void __launch_bounds__(kThreads, 1)
         // ---------------------------------------------------- epilogue
         const int etid = threadIdx.x - 64;
         const int q = warp & 3;  // TMEM lane quarter this warp may access
+        const int ch0 = ((warp - 2) >> 2) * 8;  // first of this warp's eight 8-column chunks
         const int m = q * 32 + lane;
         const int yl = m >> 1, j_own = m & 1;
-        const int zoff = j_own ? 4 : 0;
+        const int zoff = j_own ? 2 : 0;
         const BarNamed bar{1, kEpiThreads};
         const bool maximize = P.T.score == 1;
         const int M = P.D.M;
@@ -531,14 +536,14 @@ __global__ void __launch_bounds__(kThreads, 1)
                     }
                 }
             }
-            for (int ch = 0; ch < 8; ++ch) {
-                uint32_t v[4][16];
+            for (int ch = ch0; ch < ch0 + 8; ++ch) {
+                uint32_t v[4][8];
                 __syncwarp();
 #pragma unroll
                 for (int s = 0; s < 4; ++s)
-                    if (s < nseg) ptx::tmem_ld16(trow + (uint32_t)(s * 128 + ch * 16), v[s]);
+                    if (s < nseg) ptx::tmem_ld8(trow + (uint32_t)(s * 128 + ch * 8), v[s]);
                 ptx::tmem_wait_ld();
-                if (ch == 7) {
+                if (ch == ch0 + 7) {
                     ptx::tc_fence_before();
                     ptx::mbar_arrive(&tempty[b]);
                 }
@@ -546,21 +551,21 @@ __global__ void __launch_bounds__(kThreads, 1)
                 for (int s = 0; s < 4; ++s)
                     if (s >= nseg || ((emask >> s) & 1))
 #pragma unroll
-                        for (int e = 0; e < 16; ++e) v[s][e] = 0;
-                // Partner lane (other plane of the same A SNP) sends the counts of our 4 B SNPs.
-                uint32_t r[4][8];
+                        for (int e = 0; e < 8; ++e) v[s][e] = 0;
+                // Partner lane (other plane of the same A SNP) sends the counts of our 2 B SNPs.
+                uint32_t r[4][4];
 #pragma unroll
                 for (int s = 0; s < 4; ++s)
 #pragma unroll
-                    for (int e = 0; e < 8; ++e)
-                        r[s][e] = __shfl_xor_sync(0xFFFFFFFFu, j_own ? v[s][e] : v[s][8 + e], 1);
+                    for (int e = 0; e < 4; ++e)
+                        r[s][e] = __shfl_xor_sync(0xFFFFFFFFu, j_own ? v[s][e] : v[s][4 + e], 1);
                 Cand thr = *s_thr;
 #pragma unroll
-                for (int z = 0; z < 4; ++z) {
-                    const int bsnp = tl.y * kTileSnps + ch * 8 + zoff + z;
+                for (int z = 0; z < 2; ++z) {
+                    const int bsnp = tl.y * kTileSnps + ch * 4 + zoff + z;
                     // cnt(s, jj, kk): A plane jj, B plane kk, segment s
                     auto cnt = [&](int s, int jj, int kk) -> int {
-                        const uint32_t own = j_own ? v[s][8 + 2 * z + kk] : v[s][2 * z + kk];
+                        const uint32_t own = j_own ? v[s][4 + 2 * z + kk] : v[s][2 * z + kk];
                         return (int)(jj == j_own ? own : r[s][2 * z + kk]);
                     };
                     if (mode == kPairsStore) {
