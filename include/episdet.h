@@ -88,7 +88,7 @@ typedef struct episdet_cohort {
 typedef struct episdet_options {
     int32_t order;        /* 2 (pairs) or 3 (triplets) */
     int32_t score;        /* EPISDET_SCORE_K2 (minimised) or EPISDET_SCORE_MI (maximised) */
-    int32_t top_k;        /* FP32 candidates re-scored in FP64; 1..2048, default 1024 */
+    int32_t top_k;        /* FP32 candidates re-scored in FP64; 1..1536, default 1024 */
     int32_t device;       /* CUDA device ordinal, default 0 */
     int32_t engine;       /* EPISDET_ENGINE_* */
     int32_t first_begin;  /* evaluate only sets whose first SNP is in [first_begin, first_end) */

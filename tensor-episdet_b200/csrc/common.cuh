@@ -12,7 +12,7 @@
 
 namespace episdet {
 
-constexpr int kMaxTopK = 2048;
+constexpr int kMaxTopK = 1536;
 
 // Candidate: 32-bit orderable FP32 score key (smaller = better for both K2
 // and MI) and the lexicographic set key (pairs a<<32|b, triplets
@@ -68,29 +68,46 @@ struct ScoreTables {
     int score;          // 0 = K2, 1 = MI
 };
 
-// One K2 cell term, scoring.hpp:5-7: t[ctrl] + t[case] - t[ctrl+case+1].
-__device__ __forceinline__ float k2_term32(const float* __restrict__ t, int cs, int cn) {
-    return __fsub_rn(__fadd_rn(__ldg(t + cn), __ldg(t + cs)), __ldg(t + cn + cs + 1));
-}
+// The FP32 table's first kLoTab entries are also staged in shared memory by
+// the tensor epilogue; both lookups return the same value.
+constexpr int kLoTab = 8192;
 
-template <int NC>
-__device__ __forceinline__ float score32(const ScoreTables& T, const int* cs, const int* cn) {
+struct LutGlobal {
+    const float* __restrict__ t;
+    __device__ __forceinline__ float operator()(int v) const { return __ldg(t + v); }
+};
+struct LutShared {
+    const float* s_lo;  // t[0, kLoTab) in shared memory
+    const float* __restrict__ t;
+    __device__ __forceinline__ float operator()(int v) const { return v < kLoTab ? s_lo[v] : __ldg(t + v); }
+};
+
+// FP32 score of one table, scoring.hpp:5-16 (K2 cell term t[ctrl] + t[case] -
+// t[ctrl+case+1]; MI terms), cells in index order.
+template <int NC, class Lut>
+__device__ __forceinline__ float score32_lut(const ScoreTables& T, const Lut& lut, const int* cs, const int* cn) {
     if (T.score == 0) {
         float s = 0.0f;
 #pragma unroll
-        for (int c = 0; c < NC; ++c) s = __fadd_rn(s, k2_term32(T.t32, cs[c], cn[c]));
+        for (int c = 0; c < NC; ++c)
+            s = __fadd_rn(s, __fsub_rn(__fadd_rn(lut(cn[c]), lut(cs[c])), lut(cn[c] + cs[c] + 1)));
         return fabsf(s);
     }
     float ha = 0.0f, hx = 0.0f;
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
         float pc = __fmul_rn(__int2float_rn(cs[c]), T.inv_n32);
-        ha = __fmaf_rn(-pc, __ldg(T.t32 + cs[c]), ha);
+        ha = __fmaf_rn(-pc, lut(cs[c]), ha);
         float pn = __fmul_rn(__int2float_rn(cn[c]), T.inv_n32);
-        ha = __fmaf_rn(-pn, __ldg(T.t32 + cn[c]), ha);
-        hx = __fmaf_rn(-__fadd_rn(pc, pn), __ldg(T.t32 + cs[c] + cn[c]), hx);
+        ha = __fmaf_rn(-pn, lut(cn[c]), ha);
+        hx = __fmaf_rn(-__fadd_rn(pc, pn), lut(cs[c] + cn[c]), hx);
     }
     return __fsub_rn(__fadd_rn(hx, T.hy32), ha);
+}
+
+template <int NC>
+__device__ __forceinline__ float score32(const ScoreTables& T, const int* cs, const int* cn) {
+    return score32_lut<NC>(T, LutGlobal{T.t32}, cs, cn);
 }
 
 template <int NC>

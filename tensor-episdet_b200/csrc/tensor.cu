@@ -48,14 +48,14 @@ constexpr int kKB = 128;  // bytes (samples) per K block
 constexpr int kStages = 4;
 constexpr int kTileBytes = kTileRows * kKB;
 constexpr int kStageBytes = 2 * kTileBytes;
-constexpr int kCap = 4096;
+constexpr int kCap = 2048;  // k <= kMaxTopK kept plus one step of offers
 // Warp 0 issues TMA, warp 1 MMAs; warps 2..9 are the epilogue, two per TMEM
 // lane quarter (warp % 4), each taking half of the 128 accumulator columns in
 // chunks of 8 columns (4 B SNPs x 2 planes; each lane scores 2 of the 4).
 constexpr int kThreads = 320;
 constexpr int kEpiThreads = 256;
 constexpr int kEpiPerStep = kEpiThreads * 2;
-static_assert(kMaxTopK + kEpiPerStep <= 4096, "candidate buffer too small for one step of offers");
+static_assert(kMaxTopK + kEpiPerStep <= kCap, "candidate buffer too small for one step of offers");
 constexpr uint64_t kWaitLimitNs = 4000000000ull;
 constexpr uint32_t kIdesc = ptx::idesc_u8(128);
 
@@ -104,10 +104,13 @@ struct TcParams {
 };
 
 constexpr size_t kSmemTopk = (size_t)kStages * kStageBytes;
-constexpr size_t kSmemBars = kSmemTopk + (size_t)kCap * sizeof(Cand);
-constexpr size_t kSmemMisc = kSmemBars + 16 * sizeof(uint64_t);
+constexpr size_t kSmemLo = kSmemTopk + (size_t)kCap * sizeof(Cand);  // [kLoTab] float
+constexpr size_t kSmemBars = kSmemLo + (size_t)kLoTab * sizeof(float);
+constexpr int kNumBars = 2 * kStages + 5;  // full, empty, tfull[2], tempty[2], drain
+constexpr size_t kSmemMisc = kSmemBars + ((kNumBars * sizeof(uint64_t) + 63) & ~size_t(63));
 constexpr size_t kSmemGroup = kSmemMisc + 64;
 constexpr size_t kSmemTotal = kSmemGroup + 256 + 1024;
+static_assert(kSmemTotal <= 232448, "tc_kernel shared memory exceeds 227 KB");
 
 // Per-launch copy of each group member's segments in shared memory.
 struct GroupSm {
@@ -243,20 +246,32 @@ __global__ void __launch_bounds__(1024) xinfo_kernel(DevData D, int X, XInfo* in
 // Output-stationary: a CTA owns 4096 output bytes of one class region (the two
 // segments back to back) for kCmpRows rows.  Each thread keeps the source
 // sample indices of its 16 output bytes in registers and reuses them for every
-// row; the source words those samples fall in are staged in shared memory per
-// row when their span fits.  Sized (<= 64 registers, ~21 KB shared memory) so
-// that one CTA fits on an SM beside a tc_kernel CTA.
+// row.  The source words those samples fall in (one contiguous span per row)
+// are copied into a ring of kCmpDepth shared-memory buffers with cp.async,
+// kCmpDepth - 1 rows ahead of the row being gathered, so the copies of later
+// rows overlap the gathers of earlier ones.  Spans wider than kCmpSpanWords
+// (first SNPs whose kept genotypes are very rare) gather from global memory.
 constexpr int kCmpOut = 4096;
 constexpr int kCmpThreads = 256;
-constexpr int kCmpRows = 16;
-constexpr int kCmpSpanWords = 5120;
+constexpr int kCmpRows = 32;
+constexpr int kCmpSpanWords = 2048;
+constexpr int kCmpDepth = 4;
 
 __host__ __device__ inline int cmp_chunks(int words) { return (words * 32 + 256 + kCmpOut - 1) / kCmpOut; }
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(ptx::smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 __global__ void __launch_bounds__(kCmpThreads, 4)
     compact_kernel(DevData D, const XInfo* __restrict__ info, const int* __restrict__ idx, int max_n, int row0,
                    int nrows, uint8_t* __restrict__ out, int pitch) {
-    __shared__ uint32_t s_src[kCmpSpanWords];
+    __shared__ __align__(16) uint32_t s_src[kCmpDepth][kCmpSpanWords];
     __shared__ int s_lo, s_hi;
     const int C0 = cmp_chunks(D.W[0]);
     const int c = (int)blockIdx.x < C0 ? 0 : 1;
@@ -296,30 +311,54 @@ __global__ void __launch_bounds__(kCmpThreads, 4)
         atomicMax(&s_hi, hi);
     }
     __syncthreads();
-    const int wlo = s_lo, whi = s_hi;
-    const bool staged = whi >= wlo && whi - wlo + 1 <= kCmpSpanWords;
     const int W = D.W[c];
+    // Span of source words, widened to whole 16-byte groups.  Rows are W words
+    // long with W a multiple of 32, so the widened span stays inside the row.
+    const int wlo = s_lo & ~3;
+    const int nq = s_hi >= s_lo ? (s_hi - wlo + 4) >> 2 : 0;  // 16-byte groups
+    const bool staged = nq > 0 && nq * 4 <= kCmpSpanWords;
     const int colbase = (c ? D.W[0] * 32 + 256 : 0) + kk0;
     const int rbeg = row0 + (int)blockIdx.y * kCmpRows;
     const int rend = min(row0 + nrows, rbeg + kCmpRows);
-    for (int row = rbeg; row < rend; ++row) {
-        const uint32_t* srow = D.bits[c] + (size_t)row * W;
-        if (staged) {
-            for (int w = wlo + (int)threadIdx.x; w <= whi; w += kCmpThreads) s_src[w - wlo] = __ldg(srow + w);
-            __syncthreads();
-        }
-        uint32_t o[4] = {0, 0, 0, 0};
-#pragma unroll
-        for (int e = 0; e < 16; ++e) {
-            const int s = src[e];
-            if (s >= 0) {
-                const uint32_t word = staged ? s_src[(s >> 5) - wlo] : __ldg(srow + (s >> 5));
-                o[e >> 2] |= ((word >> (31 - (s & 31))) & 1u) << (8 * (e & 3));
+    const uint32_t* base = D.bits[c];
+    if (staged) {
+        auto issue = [&](int row) {
+            if (row < rend) {
+                const uint32_t* srow = base + (size_t)row * W + wlo;
+                uint32_t* dst = s_src[(row - rbeg) % kCmpDepth];
+                for (int i = (int)threadIdx.x; i < nq; i += kCmpThreads) cp_async16(dst + 4 * i, srow + 4 * i);
             }
+            cp_async_commit();  // one group per row, empty past the end
+        };
+#pragma unroll
+        for (int d = 0; d < kCmpDepth - 1; ++d) issue(rbeg + d);
+        for (int row = rbeg; row < rend; ++row) {
+            cp_async_wait<kCmpDepth - 2>();  // this thread's copies of `row` have landed
+            __syncthreads();                 // everyone's have, and the previous row's buffer is free
+            issue(row + kCmpDepth - 1);
+            const uint32_t* sw = s_src[(row - rbeg) % kCmpDepth];
+            uint32_t o[4] = {0, 0, 0, 0};
+#pragma unroll
+            for (int e = 0; e < 16; ++e) {
+                const int s = src[e];
+                if (s >= 0) o[e >> 2] |= ((sw[(s >> 5) - wlo] >> (31 - (s & 31))) & 1u) << (8 * (e & 3));
+            }
+            if (kk0 < region)
+                *reinterpret_cast<uint4*>(out + (size_t)row * pitch + colbase) = make_uint4(o[0], o[1], o[2], o[3]);
         }
-        if (kk0 < region)
-            *reinterpret_cast<uint4*>(out + (size_t)row * pitch + colbase) = make_uint4(o[0], o[1], o[2], o[3]);
-        if (staged) __syncthreads();
+        cp_async_wait<0>();
+    } else {
+        for (int row = rbeg; row < rend; ++row) {
+            const uint32_t* srow = base + (size_t)row * W;
+            uint32_t o[4] = {0, 0, 0, 0};
+#pragma unroll
+            for (int e = 0; e < 16; ++e) {
+                const int s = src[e];
+                if (s >= 0) o[e >> 2] |= ((__ldg(srow + (s >> 5)) >> (31 - (s & 31))) & 1u) << (8 * (e & 3));
+            }
+            if (kk0 < region)
+                *reinterpret_cast<uint4*>(out + (size_t)row * pitch + colbase) = make_uint4(o[0], o[1], o[2], o[3]);
+        }
     }
 }
 
@@ -332,6 +371,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* stages = smem;
     Cand* tbuf = reinterpret_cast<Cand*>(smem + kSmemTopk);
+    float* s_lo = reinterpret_cast<float*>(smem + kSmemLo);
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kSmemBars);
     uint64_t* full = bars;
     uint64_t* empty = bars + kStages;
@@ -499,13 +539,21 @@ __global__ void __launch_bounds__(kThreads, 1)
         const bool maximize = P.T.score == 1;
         const int M = P.D.M;
         LocalTopK<kCap, kEpiThreads> tk{tbuf, s_count, s_thr, P.S.k, etid};
-        if (mode != kPairsStore) tk.load(P.S.lists + (size_t)blockIdx.x * P.S.k, P.S.counts[blockIdx.x], bar);
+        const LutShared lut{s_lo, P.T.t32};
+        if (mode != kPairsStore) {
+            // Low end of the FP32 table (every index the scorer can read is < N + 2).
+            const int nlo = min(P.D.n[0] + P.D.n[1] + 2, kLoTab);
+            for (int i = etid; i < nlo; i += kEpiThreads) s_lo[i] = __ldg(P.T.t32 + i);
+            tk.load(P.S.lists + (size_t)blockIdx.x * P.S.k, P.S.counts[blockIdx.x], bar);
+        }
         bool ok = true;
         int local = 0;
         for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x, ++local) {
             const int b = local % nbuf;
             const uint32_t use = (uint32_t)(local / nbuf);
-            // The decision to leave must be uniform over the 128 epilogue
+            const int g = group_of(P, t);
+            const int2 tl = P.grp[g].tiles[t - P.grp[g].cum];
+            // The decision to leave must be uniform over the 256 epilogue
             // threads (they meet at named barriers), so it is taken after a
             // barrier from a flag only they write.
             if (!ptx::mbar_wait(&tfull[b], use & 1, abort, kWaitLimitNs)) *s_epi_fail = 1;
@@ -515,8 +563,6 @@ __global__ void __launch_bounds__(kThreads, 1)
                 break;
             }
             ptx::tc_fence_after();
-            const int g = group_of(P, t);
-            const int2 tl = P.grp[g].tiles[t - P.grp[g].cum];
             const int ga = s_grp[g].ga, gb = s_grp[g].gb, emask = s_grp[g].empty_mask;
             const int arow = tl.x * kTileSnps + yl;  // this thread's A SNP (pairs: a, triplets: Y)
             const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * nseg * 128);
@@ -592,7 +638,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                         cn[4] = cnt(1, 1, 1);
                         load_marg3(P.D.marg[1], M, bsnp, mb);
                         derive9(cn, ma[1], mb);
-                        float sc = score32<9>(P.T, cs, cn);
+                        float sc = score32_lut<9>(P.T, lut, cs, cn);
                         Cand cd;
                         cd.key = score_key(sc, maximize);
                         cd.pad = 0;
@@ -622,7 +668,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                         pair9_from4(yz9, yz, ma[c], mz);
                         derive27(tab[c], xy9[c], xz9, yz9);
                     }
-                    float sc = score32<27>(P.T, tab[0], tab[1]);
+                    float sc = score32_lut<27>(P.T, lut, tab[0], tab[1]);
                     Cand cd;
                     cd.key = score_key(sc, maximize);
                     cd.pad = 0;

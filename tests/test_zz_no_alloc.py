@@ -42,7 +42,7 @@ def test_noalloc_rejects_oversize_and_host_inputs(episdet):
     dc = torch.from_numpy(cases.view(np.int32)).cuda()
     dn = torch.from_numpy(controls.view(np.int32)).cuda()
     with pytest.raises(episdet.EpisdetError) as e:
-        episdet.search_pairs_noalloc(dc, dn, 500, 500, num_snps=64, top_k=2048)
+        episdet.search_pairs_noalloc(dc, dn, 500, 500, num_snps=64, top_k=1200)
     assert "no-alloc limits" in str(e.value)
     big = torch.zeros((4097 * 2 * 32,), dtype=torch.int32, device="cuda")
     with pytest.raises(episdet.EpisdetError) as e:
