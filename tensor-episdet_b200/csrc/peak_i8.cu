@@ -27,7 +27,9 @@ constexpr uint64_t kLimitNs = 2000000000ull;
 
 __device__ int g_err;
 
-// mode 0: MMA only; mode 1: MMA plus a concurrent TMA stream into a separate buffer.
+// mode 0: MMA only, accumulators alternating every 4 MMAs; mode 1: mode 0 plus a
+// concurrent TMA stream into a separate buffer; mode 2: every MMA into one
+// accumulator; mode 3: accumulators rotating every MMA over 512 / N regions.
 template <int N>
 __global__ void __launch_bounds__(kThreads, 1)
     peak_kernel(const __grid_constant__ CUtensorMap map, int iters, int mode, unsigned long long* cycles) {
@@ -76,7 +78,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
             for (int m = 0; m < 16; ++m) {
                 const int kk = m & 3;
-                ptx::mma_u8(tmem + (uint32_t)((m >> 2) & 1) * N, ad + 2 * kk, bd + 2 * kk, idesc, 1u);
+                const uint32_t acc = mode == 2 ? 0u : (mode == 3 ? (uint32_t)(m % (512 / N)) : (uint32_t)((m >> 2) & 1));
+                ptx::mma_u8(tmem + acc * N, ad + 2 * kk, bd + 2 * kk, idesc, 1u);
             }
             ptx::mma_commit(&bars[slot]);
         }
@@ -148,7 +151,7 @@ static int run(const CUtensorMap& map, int sms, int iters, int mode, unsigned lo
     CK(cudaMemcpy(&cyc, d_cyc, sizeof(cyc), cudaMemcpyDeviceToHost));
     printf("{\"n\": %d, \"mode\": \"%s\", \"ms\": %.3f, \"tmacs_per_s\": %.1f, \"tops\": %.1f, "
            "\"mac_per_clk_per_sm\": %.0f, \"err\": %d}\n",
-           N, mode ? "mma+tma_stream" : "mma_only", ms, macs / (ms * 1e-3) / 1e12, 2 * macs / (ms * 1e-3) / 1e12,
+           N, mode == 1 ? "mma+tma_stream" : (mode == 2 ? "one_accumulator" : (mode == 3 ? "rotating_accumulators" : "mma_only")), ms, macs / (ms * 1e-3) / 1e12, 2 * macs / (ms * 1e-3) / 1e12,
            (double)iters * 16.0 * 128.0 * N * 32.0 / (double)cyc, err);
     (void)clock_ghz;
     return err;
@@ -190,5 +193,9 @@ int main(int argc, char** argv) {
     rc |= run<256>(map, p.multiProcessorCount, iters, 0, d_cyc, 0);
     rc |= run<128>(map, p.multiProcessorCount, iters, 1, d_cyc, 0);
     rc |= run<256>(map, p.multiProcessorCount, iters, 1, d_cyc, 0);
+    for (int mode = 2; mode <= 3; ++mode) {
+        rc |= run<128>(map, p.multiProcessorCount, iters, mode, d_cyc, 0);
+        rc |= run<256>(map, p.multiProcessorCount, iters, mode, d_cyc, 0);
+    }
     return rc;
 }

@@ -181,10 +181,26 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* s_warp, int* tot
 
 // Per first SNP X and class: which genotype of X to derive (the most frequent
 // over both classes), and the ascending sample indices of the two kept ones.
-__global__ void __launch_bounds__(1024) xinfo_kernel(DevData D, int X, XInfo* info, int* idx, int max_n) {
+// Regrouping work of the first SNPs X0 .. X0 + gridDim.y - 1 of one launch: member
+// m = blockIdx.y owns the XInfo and index lists at base + m * stride bytes.
+struct XWork {
+    uint8_t* base;     // member 0's XInfo, its index lists info_bytes after it
+    size_t stride;     // bytes between members
+    size_t info_bytes;
+    int x0;
+    int max_n;
+    __device__ __forceinline__ XInfo* info(int m) const { return reinterpret_cast<XInfo*>(base + m * stride); }
+    __device__ __forceinline__ int* idx(int m) const { return reinterpret_cast<int*>(base + m * stride + info_bytes); }
+};
+
+__global__ void __launch_bounds__(1024) xinfo_kernel(DevData D, XWork xw) {
     __shared__ int s_warp[32];
     __shared__ int s_total;
     const int c = blockIdx.x;
+    const int X = xw.x0 + (int)blockIdx.y;
+    XInfo* info = xw.info(blockIdx.y);
+    int* idx = xw.idx(blockIdx.y);
+    const int max_n = xw.max_n;
     const int M = D.M;
     int tot[3];
 #pragma unroll
@@ -268,11 +284,24 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// Output rows of the members of one launch: member m = blockIdx.z writes rows
+// [row0[m], nrows_total) of out[m].
+struct CmpOut {
+    uint8_t* out[kMaxGroup];
+    int row0[kMaxGroup];
+};
+
 __global__ void __launch_bounds__(kCmpThreads, 4)
-    compact_kernel(DevData D, const XInfo* __restrict__ info, const int* __restrict__ idx, int max_n, int row0,
-                   int nrows, uint8_t* __restrict__ out, int pitch) {
+    compact_kernel(DevData D, XWork xw, CmpOut co, int rows_total, int pitch) {
     __shared__ __align__(16) uint32_t s_src[kCmpDepth][kCmpSpanWords];
     __shared__ int s_lo, s_hi;
+    const int mem = (int)blockIdx.z;
+    const XInfo* __restrict__ info = xw.info(mem);
+    const int* __restrict__ idx = xw.idx(mem);
+    const int max_n = xw.max_n;
+    const int row0 = co.row0[mem], nrows = rows_total - row0;
+    uint8_t* __restrict__ out = co.out[mem];
+    if ((int)blockIdx.y * kCmpRows >= nrows) return;  // uniform over the CTA
     const int C0 = cmp_chunks(D.W[0]);
     const int c = (int)blockIdx.x < C0 ? 0 : 1;
     const int chunk = (int)blockIdx.x - (c ? C0 : 0);
@@ -846,12 +875,18 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     TmapPack tmx;
     memset(&tmx, 0, sizeof(tmx));
     XInfo* d_info[kMaxGroup];
-    int* d_idx[kMaxGroup];
+    XWork xw;
+    xw.base = (uint8_t*)w->xinfo.p;
+    xw.stride = info_bytes + idx_bytes;
+    xw.info_bytes = info_bytes;
+    xw.max_n = max_n;
+    CmpOut co;
     for (int i = 0; i < kMaxGroup; ++i) {
         st = make_tmap(&tmx.m[i], w->xsub[i].p, (uint64_t)rows, (uint64_t)pitchx);
         if (st != EPISDET_OK) return st;
-        d_info[i] = (XInfo*)((uint8_t*)w->xinfo.p + i * (info_bytes + idx_bytes));
-        d_idx[i] = (int*)((uint8_t*)d_info[i] + info_bytes);
+        d_info[i] = (XInfo*)(xw.base + i * xw.stride);
+        co.out[i] = (uint8_t*)w->xsub[i].p;
+        co.row0[i] = 0;
     }
     std::vector<int> off((size_t)nt + 1, 0);
     for (int t = 0; t < nt; ++t) off[t + 1] = off[t] + (nt - t);
@@ -859,22 +894,23 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     p.mode = kTriplets;
     for (int x0 = fb; x0 < xend; x0 += kMaxGroup) {
         const int gn = std::min(kMaxGroup, xend - x0);
+        // Index lists and regrouped rows of the gn first SNPs, one launch each.
+        xw.x0 = x0;
+        xinfo_kernel<<<dim3(2, gn), 1024, 0, w->st>>>(D, xw);
+        CHECK_LAUNCH();
+        for (int g = 0; g < gn; ++g) co.row0[g] = 2 * ((x0 + g + 1) / kTileSnps) * kTileSnps;
+        const int max_rows = rows - co.row0[0];  // the first member needs the most rows
+        const dim3 cgrid(cmp_chunks(D.W[0]) + cmp_chunks(D.W[1]), (max_rows + kCmpRows - 1) / kCmpRows, gn);
+        compact_kernel<<<cgrid, kCmpThreads, 0, w->st>>>(D, xw, co, rows, pitchx);
+        CHECK_LAUNCH();
+        *launches += 2;
         int cum = 0;
         for (int g = 0; g < gn; ++g) {
             const int x = x0 + g;
             if (progress && x % 256 == 0) printf("Outer loop iteration %d out of %d\n", x / 256, bs_lines);
             const int t0 = (x + 1) / kTileSnps;
-            xinfo_kernel<<<2, 1024, 0, w->st>>>(D, x, d_info[g], d_idx[g], max_n);
-            CHECK_LAUNCH();
-            const int row0 = 2 * t0 * kTileSnps;
-            const int nrows = rows - row0;
-            const dim3 cgrid(cmp_chunks(D.W[0]) + cmp_chunks(D.W[1]), (nrows + kCmpRows - 1) / kCmpRows);
-            compact_kernel<<<cgrid, kCmpThreads, 0, w->st>>>(D, d_info[g], d_idx[g], max_n, row0, nrows,
-                                                              (uint8_t*)w->xsub[g].p, pitchx);
-            CHECK_LAUNCH();
             p.grp[g] = GroupDesc{d_lists + list_off[t0], cum, x, d_info[g]};
             cum += off[nt] - off[t0];
-            *launches += 2;
         }
         p.ngroup = gn;
         p.ntiles = cum;
