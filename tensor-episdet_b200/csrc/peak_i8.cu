@@ -29,7 +29,8 @@ __device__ int g_err;
 
 // mode 0: MMA only, accumulators alternating every 4 MMAs; mode 1: mode 0 plus a
 // concurrent TMA stream into a separate buffer; mode 2: every MMA into one
-// accumulator; mode 3: accumulators rotating every MMA over 512 / N regions.
+// accumulator; mode 3: accumulators rotating every MMA over 512 / N regions;
+// mode 4: as mode 0 but a commit after every 4 MMAs (the engine's stage size).
 template <int N>
 __global__ void __launch_bounds__(kThreads, 1)
     peak_kernel(const __grid_constant__ CUtensorMap map, int iters, int mode, unsigned long long* cycles) {
@@ -38,15 +39,16 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint8_t* a = sm;                      // 128 x 128 bytes
     uint8_t* b = sm + 16384;              // N x 128 bytes
     uint8_t* stream = b + N * 128;        // 2 x 32 KB landing zone of the TMA stream
-    uint64_t* bars = reinterpret_cast<uint64_t*>(stream + 65536);  // [0..3] mma ring, [4..5] tma, [6] drain
-    uint32_t* s_tmem = reinterpret_cast<uint32_t*>(bars + 8);
+    // [0..15] commit ring, [16..17] TMA stream, [18] drain
+    uint64_t* bars = reinterpret_cast<uint64_t*>(stream + 65536);
+    uint32_t* s_tmem = reinterpret_cast<uint32_t*>(bars + 20);
     int* s_abort = reinterpret_cast<int*>(s_tmem + 1);
     int* s_never = s_abort + 1;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int i = threadIdx.x; i < (16384 + N * 128) / 4; i += kThreads)
         reinterpret_cast<uint32_t*>(sm)[i] = (i * 2654435761u) & 0x01010101u;
     if (threadIdx.x == 0) {
-        for (int i = 0; i < 7; ++i) ptx::mbar_init(&bars[i], 1);
+        for (int i = 0; i < 19; ++i) ptx::mbar_init(&bars[i], 1);
         *s_abort = 0;
         *s_never = 0;
         ptx::fence_barrier_init();
@@ -65,26 +67,29 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint32_t idesc = ptx::idesc_u8(N);
         const uint64_t ad = ptx::smem_desc_sw128(ptx::smem_u32(a)), bd = ptx::smem_desc_sw128(ptx::smem_u32(b));
         long long t0 = clock64();
-        uint32_t ph[4] = {0, 0, 0, 0};
-        for (int it = 0; it < iters; ++it) {
-            const int slot = it & 3;
-            if (it >= 4) {  // keep at most 4 groups of 16 MMAs in flight
-                if (!ptx::mbar_wait(&bars[slot], ph[slot], abort, kLimitNs)) {
+        // Groups of G MMAs, one commit each; at most 64 MMAs in flight.
+        const int G = mode == 4 ? 4 : 16, ring = 64 / G, groups = iters * (16 / G);
+        uint32_t ph = 0;  // parity bits of the ring's barriers
+        for (int it = 0; it < groups; ++it) {
+            const int slot = it % ring;
+            if (it >= ring) {
+                if (!ptx::mbar_wait(&bars[slot], (ph >> slot) & 1u, abort, kLimitNs)) {
                     atomicExch(&g_err, 1);
                     *s_abort = 1;
                     break;
                 }
-                ph[slot] ^= 1;
+                ph ^= 1u << slot;
             }
-            for (int m = 0; m < 16; ++m) {
+            for (int m0 = 0; m0 < G; ++m0) {
+                const int m = (it * G + m0) & 15;
                 const int kk = m & 3;
                 const uint32_t acc = mode == 2 ? 0u : (mode == 3 ? (uint32_t)(m % (512 / N)) : (uint32_t)((m >> 2) & 1));
                 ptx::mma_u8(tmem + acc * N, ad + 2 * kk, bd + 2 * kk, idesc, 1u);
             }
             ptx::mma_commit(&bars[slot]);
         }
-        ptx::mma_commit(&bars[6]);
-        if (!ptx::mbar_wait(&bars[6], 0, s_never, kLimitNs)) atomicExch(&g_err, 2);
+        ptx::mma_commit(&bars[18]);
+        if (!ptx::mbar_wait(&bars[18], 0, s_never, kLimitNs)) atomicExch(&g_err, 2);
         cycles[blockIdx.x] = (unsigned long long)(clock64() - t0);
         *s_abort = 1;  // stops the TMA stream
     } else if (warp == 2 && lane == 0 && mode == 1) {
@@ -93,20 +98,20 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int it = 0; !*abort; ++it) {
             const int s = it & 1;
             if (issued[s]) {
-                if (!ptx::mbar_wait(&bars[4 + s], ph[s], s_never, kLimitNs)) {
+                if (!ptx::mbar_wait(&bars[16 + s], ph[s], s_never, kLimitNs)) {
                     atomicExch(&g_err, 3);
                     break;
                 }
                 ph[s] ^= 1;
             }
-            ptx::mbar_arrive_expect_tx(&bars[4 + s], 32768);
+            ptx::mbar_arrive_expect_tx(&bars[16 + s], 32768);
             const int row = ((blockIdx.x * 7 + it) % 64) * 128;
-            ptx::tma_load_2d(stream + s * 32768, &map, 0, row, &bars[4 + s]);
-            ptx::tma_load_2d(stream + s * 32768 + 16384, &map, 128, row, &bars[4 + s]);
+            ptx::tma_load_2d(stream + s * 32768, &map, 0, row, &bars[16 + s]);
+            ptx::tma_load_2d(stream + s * 32768 + 16384, &map, 128, row, &bars[16 + s]);
             issued[s] = true;
         }
         for (int s = 0; s < 2; ++s)
-            if (issued[s] && !ptx::mbar_wait(&bars[4 + s], ph[s], s_never, kLimitNs)) atomicExch(&g_err, 4);
+            if (issued[s] && !ptx::mbar_wait(&bars[16 + s], ph[s], s_never, kLimitNs)) atomicExch(&g_err, 4);
     }
     ptx::tc_fence_before();
     __syncthreads();
@@ -151,7 +156,7 @@ static int run(const CUtensorMap& map, int sms, int iters, int mode, unsigned lo
     CK(cudaMemcpy(&cyc, d_cyc, sizeof(cyc), cudaMemcpyDeviceToHost));
     printf("{\"n\": %d, \"mode\": \"%s\", \"ms\": %.3f, \"tmacs_per_s\": %.1f, \"tops\": %.1f, "
            "\"mac_per_clk_per_sm\": %.0f, \"err\": %d}\n",
-           N, mode == 1 ? "mma+tma_stream" : (mode == 2 ? "one_accumulator" : (mode == 3 ? "rotating_accumulators" : "mma_only")), ms, macs / (ms * 1e-3) / 1e12, 2 * macs / (ms * 1e-3) / 1e12,
+           N, mode == 1 ? "mma+tma_stream" : (mode == 2 ? "one_accumulator" : (mode == 3 ? "rotating_accumulators" : (mode == 4 ? "commit_every_4" : "mma_only"))), ms, macs / (ms * 1e-3) / 1e12, 2 * macs / (ms * 1e-3) / 1e12,
            (double)iters * 16.0 * 128.0 * N * 32.0 / (double)cyc, err);
     (void)clock_ghz;
     return err;
@@ -193,7 +198,9 @@ int main(int argc, char** argv) {
     rc |= run<256>(map, p.multiProcessorCount, iters, 0, d_cyc, 0);
     rc |= run<128>(map, p.multiProcessorCount, iters, 1, d_cyc, 0);
     rc |= run<256>(map, p.multiProcessorCount, iters, 1, d_cyc, 0);
-    for (int mode = 2; mode <= 3; ++mode) {
+    rc |= run<64>(map, p.multiProcessorCount, iters, 0, d_cyc, 0);
+    rc |= run<64>(map, p.multiProcessorCount, iters, 4, d_cyc, 0);
+    for (int mode = 2; mode <= 4; ++mode) {
         rc |= run<128>(map, p.multiProcessorCount, iters, mode, d_cyc, 0);
         rc |= run<256>(map, p.multiProcessorCount, iters, mode, d_cyc, 0);
     }

@@ -45,9 +45,7 @@ namespace tc {
 constexpr int kTileSnps = 64;
 constexpr int kTileRows = 128;
 constexpr int kKB = 128;  // bytes (samples) per K block
-constexpr int kStages = 4;
-constexpr int kTileBytes = kTileRows * kKB;
-constexpr int kStageBytes = 2 * kTileBytes;
+constexpr int kTileBytes = kTileRows * kKB;  // one 128-row operand tile of one K block
 constexpr int kCap = 2048;  // k <= kMaxTopK kept plus one step of offers
 // Warp 0 issues TMA, warp 1 MMAs; warps 2..9 are the epilogue, two per TMEM
 // lane quarter (warp % 4), each taking half of the 128 accumulator columns in
@@ -58,6 +56,7 @@ constexpr int kEpiPerStep = kEpiThreads * 2;
 static_assert(kMaxTopK + kEpiPerStep <= kCap, "candidate buffer too small for one step of offers");
 constexpr uint64_t kWaitLimitNs = 4000000000ull;
 constexpr uint32_t kIdesc = ptx::idesc_u8(128);
+constexpr uint32_t kIdescPair = ptx::idesc_u8(128, 256);  // CTA-pair MMA, M = 256
 
 enum Mode { kPairsScore = 0, kPairsStore = 1, kTriplets = 2 };
 
@@ -75,9 +74,11 @@ struct XInfo {
 constexpr int kMaxGroup = 4;  // first SNPs (X) per triplet launch
 constexpr int kBand = 12;     // tile-band edge of the triplet tile order
 
-// One tensor map per X of a launch (each X has its own regrouped operand rows).
+// Tensor maps of a launch, one per X (each X has its own regrouped operand
+// rows): m[g] reads 128-row boxes; the CTA-pair kernel also uses m[kMaxGroup + g],
+// 64-row boxes of the same rows for its half of the B operand.
 struct TmapPack {
-    CUtensorMap m[kMaxGroup];
+    CUtensorMap m[2 * kMaxGroup];
 };
 
 // Tiles [cum, next cum) of a launch belong to group member g: X = x, list tiles.
@@ -103,14 +104,24 @@ struct TcParams {
     int* err;
 };
 
-constexpr size_t kSmemTopk = (size_t)kStages * kStageBytes;
-constexpr size_t kSmemLo = kSmemTopk + (size_t)kCap * sizeof(Cand);  // [kLoTab] float
-constexpr size_t kSmemBars = kSmemLo + (size_t)kLoTab * sizeof(float);
-constexpr int kNumBars = 2 * kStages + 5;  // full, empty, tfull[2], tempty[2], drain
-constexpr size_t kSmemMisc = kSmemBars + ((kNumBars * sizeof(uint64_t) + 63) & ~size_t(63));
-constexpr size_t kSmemGroup = kSmemMisc + 64;
-constexpr size_t kSmemTotal = kSmemGroup + 256 + 1024;
-static_assert(kSmemTotal <= 232448, "tc_kernel shared memory exceeds 227 KB");
+// Shared-memory layout of tc_kernel<PAIR>.  A stage holds one K block of this
+// CTA's 128 A rows and of its B rows: all 128 for one CTA, 64 for a CTA pair
+// (PAIR), where the other CTA of the pair holds the other 64.
+template <bool PAIR>
+struct Cfg {
+    static constexpr int kStages = PAIR ? 5 : 4;
+    static constexpr int kBRows = PAIR ? 64 : 128;
+    static constexpr int kStageBytes = kTileBytes + kBRows * kKB;
+    static constexpr size_t kSmemTopk = (size_t)kStages * kStageBytes;
+    static constexpr size_t kSmemLo = kSmemTopk + (size_t)kCap * sizeof(Cand);  // [kLoTab] float
+    static constexpr size_t kSmemBars = kSmemLo + (size_t)kLoTab * sizeof(float);
+    static constexpr int kNumBars = 2 * kStages + 5;  // full, empty, tfull[2], tempty[2], drain
+    static constexpr size_t kSmemMisc = kSmemBars + ((kNumBars * sizeof(uint64_t) + 63) & ~size_t(63));
+    static constexpr size_t kSmemGroup = kSmemMisc + 64;
+    static constexpr size_t kSmemTotal = kSmemGroup + 256 + 1024;
+    static_assert(kSmemTotal <= 232448, "tc_kernel shared memory exceeds 227 KB");
+    static_assert(kStageBytes % 1024 == 0, "operand tiles must stay 1024-byte aligned");
+};
 
 // Per-launch copy of each group member's segments in shared memory.
 struct GroupSm {
@@ -394,29 +405,36 @@ __global__ void __launch_bounds__(kCmpThreads, 4)
 __device__ __forceinline__ void record_error(int* err, int code) { atomicCAS(err, 0, code); }
 
 // ------------------------------------------------------------------ kernel
+// PAIR: launched as clusters of two CTAs that share each M = 256 x N = 128
+// tile (cta_group::2): the even CTA's MMA warp issues for both, each CTA holds
+// the accumulators of its 128 A rows and scores them.  Triplet mode only.
+template <bool PAIR>
 __global__ void __launch_bounds__(kThreads, 1)
     tc_kernel(const __grid_constant__ TmapPack tm, const __grid_constant__ TcParams P) {
+    using C = Cfg<PAIR>;
+    constexpr int kStages = C::kStages;
+    constexpr int kStageBytes = C::kStageBytes;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* stages = smem;
-    Cand* tbuf = reinterpret_cast<Cand*>(smem + kSmemTopk);
-    float* s_lo = reinterpret_cast<float*>(smem + kSmemLo);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kSmemBars);
+    Cand* tbuf = reinterpret_cast<Cand*>(smem + C::kSmemTopk);
+    float* s_lo = reinterpret_cast<float*>(smem + C::kSmemLo);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + C::kSmemBars);
     uint64_t* full = bars;
     uint64_t* empty = bars + kStages;
     uint64_t* tfull = bars + 2 * kStages;
     uint64_t* tempty = bars + 2 * kStages + 2;
     uint64_t* drain = bars + 2 * kStages + 4;
-    uint32_t* s_tmem = reinterpret_cast<uint32_t*>(smem + kSmemMisc);
-    int* s_abort = reinterpret_cast<int*>(smem + kSmemMisc + 4);
-    int* s_never = reinterpret_cast<int*>(smem + kSmemMisc + 8);  // stays 0: drain waits ignore aborts
-    int* s_epi_fail = reinterpret_cast<int*>(smem + kSmemMisc + 12);
-    int* s_count = reinterpret_cast<int*>(smem + kSmemMisc + 16);
-    Cand* s_thr = reinterpret_cast<Cand*>(smem + kSmemMisc + 32);
+    uint32_t* s_tmem = reinterpret_cast<uint32_t*>(smem + C::kSmemMisc);
+    int* s_abort = reinterpret_cast<int*>(smem + C::kSmemMisc + 4);
+    int* s_never = reinterpret_cast<int*>(smem + C::kSmemMisc + 8);  // stays 0: drain waits ignore aborts
+    int* s_epi_fail = reinterpret_cast<int*>(smem + C::kSmemMisc + 12);
+    int* s_count = reinterpret_cast<int*>(smem + C::kSmemMisc + 16);
+    Cand* s_thr = reinterpret_cast<Cand*>(smem + C::kSmemMisc + 32);
     volatile int* abort = s_abort;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    GroupSm* s_grp = reinterpret_cast<GroupSm*>(smem + kSmemGroup);
+    GroupSm* s_grp = reinterpret_cast<GroupSm*>(smem + C::kSmemGroup);
     const int mode = P.mode;
     const int nseg = mode == kTriplets ? 4 : 2;
     const int nbuf = 4 / nseg;
@@ -448,7 +466,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         for (int b = 0; b < 2; ++b) {
             ptx::mbar_init(&tfull[b], 1);
-            ptx::mbar_init(&tempty[b], kEpiThreads);
+            ptx::mbar_init(&tempty[b], PAIR ? 2 * (kEpiThreads / 32) : kEpiThreads);
         }
         ptx::mbar_init(drain, 1);
         *s_abort = 0;
@@ -457,14 +475,29 @@ __global__ void __launch_bounds__(kThreads, 1)
         ptx::fence_barrier_init();
     }
     if (warp == 1) {
-        ptx::tmem_alloc(s_tmem, 512);
-        ptx::tmem_relinquish();
+        if constexpr (PAIR) {
+            ptx::tmem_alloc_pair(s_tmem, 512);
+            ptx::tmem_relinquish_pair();
+        } else {
+            ptx::tmem_alloc(s_tmem, 512);
+            ptx::tmem_relinquish();
+        }
     }
-    if (warp == 0 && lane < P.ngroup) ptx::prefetch_tmap(&tm.m[lane]);
+    if (warp == 0 && lane < P.ngroup) {
+        ptx::prefetch_tmap(&tm.m[lane]);
+        if (PAIR) ptx::prefetch_tmap(&tm.m[kMaxGroup + lane]);
+    }
+    // The pair's barriers must be initialised before either CTA touches the other's.
     ptx::tc_fence_before();
-    __syncthreads();
+    if constexpr (PAIR)
+        ptx::cluster_sync();
+    else
+        __syncthreads();
     ptx::tc_fence_after();
     const uint32_t tmem = *s_tmem;
+    const int rank = PAIR ? (int)ptx::cluster_ctarank() : 0;
+    const int t_first = PAIR ? (int)ptx::cluster_id_x() : (int)blockIdx.x;
+    const int t_step = PAIR ? (int)ptx::nclusters_x() : (int)gridDim.x;
 
     if (warp == 0) {
         // ---------------------------------------------------- TMA producer
@@ -477,23 +510,37 @@ __global__ void __launch_bounds__(kThreads, 1)
                 pend[i] = false;
                 pend_phase[i] = 0;
             }
-            bool ok = true;
-            for (int t = blockIdx.x; ok && t < P.ntiles; t += gridDim.x) {
+            bool ok = true, issued = false;
+            // The even CTA arms each stage's full barrier for both CTAs' bytes;
+            // the odd CTA's copies count on that barrier too.
+            const uint32_t full0 = PAIR ? ptx::mapa(full, 0) : 0u;
+            for (int t = t_first; ok && t < P.ntiles; t += t_step) {
                 const int g = group_of(P, t);
                 const int2 tl = P.grp[g].tiles[t - P.grp[g].cum];
                 const Seg* seg = s_grp[g].seg;
                 const CUtensorMap* tmap = &tm.m[g];
+                const CUtensorMap* tmapb = PAIR ? &tm.m[kMaxGroup + g] : tmap;
+                const int arow0 = PAIR ? tl.x * 2 * kTileRows + rank * kTileRows : tl.x * kTileRows;
+                const int brow0 = PAIR ? tl.y * kTileRows + rank * C::kBRows : tl.y * kTileRows;
                 for (int s = 0; ok && s < nseg; ++s)
                     for (int kb = seg[s].kb0; kb < seg[s].kb1; ++kb) {
                         if (!ptx::mbar_wait(&empty[stage], phase ^ 1, abort, kWaitLimitNs)) {
                             ok = false;
                             break;
                         }
-                        ptx::mbar_arrive_expect_tx(&full[stage], kStageBytes);
                         uint8_t* sa = stages + (size_t)stage * kStageBytes;
-                        ptx::tma_load_2d(sa, tmap, kb * kKB, tl.x * kTileRows, &full[stage]);
-                        ptx::tma_load_2d(sa + kTileBytes, tmap, kb * kKB, tl.y * kTileRows, &full[stage]);
-                        pend[stage] = true;
+                        if constexpr (PAIR) {
+                            if (rank == 0) ptx::mbar_arrive_expect_tx(&full[stage], 2 * kStageBytes);
+                            const uint32_t fb = full0 + (uint32_t)(stage * sizeof(uint64_t));
+                            ptx::tma_load_2d_pair(sa, tmap, kb * kKB, arow0, fb);
+                            ptx::tma_load_2d_pair(sa + kTileBytes, tmapb, kb * kKB, brow0, fb);
+                        } else {
+                            ptx::mbar_arrive_expect_tx(&full[stage], kStageBytes);
+                            ptx::tma_load_2d(sa, tmap, kb * kKB, arow0, &full[stage]);
+                            ptx::tma_load_2d(sa + kTileBytes, tmapb, kb * kKB, brow0, &full[stage]);
+                        }
+                        issued = true;
+                        pend[stage] = !PAIR || rank == 0;  // completions land on the even CTA's barriers
                         pend_phase[stage] = phase;
                         if (++stage == kStages) {
                             stage = 0;
@@ -504,23 +551,33 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (!ok) {
                 record_error(P.err, 1);
                 *s_abort = 1;
+                // The odd CTA cannot observe its copies; give any still in
+                // flight time to land (they complete within microseconds).
+                if (PAIR && rank != 0 && issued) {
+                    const uint64_t t0 = ptx::globaltimer();
+                    while (ptx::globaltimer() - t0 < 200000ull) __nanosleep(1000);
+                }
             }
-            // Never leave with a copy in flight.
+            // Never leave with a copy in flight (the even CTA's barriers count both CTAs' copies).
             for (int i = 0; i < kStages; ++i)
                 if (pend[i] && !ptx::mbar_wait(&full[i], pend_phase[i], s_never, kWaitLimitNs))
                     record_error(P.err, 2);
         }
     } else if (warp == 1) {
         // ---------------------------------------------------- MMA issuer
-        if (lane == 0) {
+        // (for a CTA pair, the even CTA issues every MMA of the pair)
+        if (lane == 0 && rank == 0) {
             uint32_t stage = 0, phase = 0;
             bool ok = true;
             int local = 0;
-            for (int t = blockIdx.x; ok && t < P.ntiles; t += gridDim.x, ++local) {
+            for (int t = t_first; ok && t < P.ntiles; t += t_step, ++local) {
                 const Seg* seg = s_grp[group_of(P, t)].seg;
                 const int b = local % nbuf;
                 const uint32_t use = (uint32_t)(local / nbuf);
-                if (!ptx::mbar_wait(&tempty[b], (use & 1) ^ 1, abort, kWaitLimitNs)) {
+                // Both CTAs' epilogues must have drained accumulator set b.
+                const bool freed = PAIR ? ptx::mbar_wait_cluster(&tempty[b], (use & 1) ^ 1, abort, kWaitLimitNs)
+                                        : ptx::mbar_wait(&tempty[b], (use & 1) ^ 1, abort, kWaitLimitNs);
+                if (!freed) {
                     ok = false;
                     break;
                 }
@@ -536,23 +593,38 @@ __global__ void __launch_bounds__(kThreads, 1)
                         const uint32_t sa = ptx::smem_u32(stages + (size_t)stage * kStageBytes);
                         const uint64_t ad = ptx::smem_desc_sw128(sa), bd = ptx::smem_desc_sw128(sa + kTileBytes);
 #pragma unroll
-                        for (int kk = 0; kk < kKB / 32; ++kk)
-                            ptx::mma_u8(dbase + (uint32_t)(s * 128), ad + 2 * kk, bd + 2 * kk, kIdesc,
-                                        (kb > seg[s].kb0 || kk > 0) ? 1u : 0u);
-                        ptx::mma_commit(&empty[stage]);
+                        for (int kk = 0; kk < kKB / 32; ++kk) {
+                            const uint32_t acc = (kb > seg[s].kb0 || kk > 0) ? 1u : 0u;
+                            if constexpr (PAIR)
+                                ptx::mma_u8_pair(dbase + (uint32_t)(s * 128), ad + 2 * kk, bd + 2 * kk, kIdescPair, acc);
+                            else
+                                ptx::mma_u8(dbase + (uint32_t)(s * 128), ad + 2 * kk, bd + 2 * kk, kIdesc, acc);
+                        }
+                        if constexpr (PAIR)
+                            ptx::mma_commit_pair_mc(&empty[stage], 0x3);  // frees the stage in both CTAs
+                        else
+                            ptx::mma_commit(&empty[stage]);
                         if (++stage == kStages) {
                             stage = 0;
                             phase ^= 1;
                         }
                     }
-                if (ok) ptx::mma_commit(&tfull[b]);
+                if (ok) {
+                    if constexpr (PAIR)
+                        ptx::mma_commit_pair_mc(&tfull[b], 0x3);
+                    else
+                        ptx::mma_commit(&tfull[b]);
+                }
             }
             if (!ok) {
                 record_error(P.err, 3);
                 *s_abort = 1;
             }
             // Every MMA this thread issued completes before TMEM is released.
-            ptx::mma_commit(drain);
+            if constexpr (PAIR)
+                ptx::mma_commit_pair_mc(drain, 0x1);
+            else
+                ptx::mma_commit(drain);
             if (!ptx::mbar_wait(drain, 0, s_never, kWaitLimitNs))
                 record_error(P.err, 4);
         }
@@ -577,7 +649,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         bool ok = true;
         int local = 0;
-        for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x, ++local) {
+        for (int t = t_first; t < P.ntiles; t += t_step, ++local) {
             const int b = local % nbuf;
             const uint32_t use = (uint32_t)(local / nbuf);
             const int g = group_of(P, t);
@@ -593,7 +665,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
             ptx::tc_fence_after();
             const int ga = s_grp[g].ga, gb = s_grp[g].gb, emask = s_grp[g].empty_mask;
-            const int arow = tl.x * kTileSnps + yl;  // this thread's A SNP (pairs: a, triplets: Y)
+            // This thread's A SNP (pairs: a, triplets: Y); a pair tile spans 128 A SNPs.
+            const int arow = PAIR ? tl.x * 2 * kTileSnps + rank * kTileSnps + yl : tl.x * kTileSnps + yl;
             const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * nseg * 128);
             // Per-row constants.
             int ma[2][3] = {{0, 0, 0}, {0, 0, 0}}, mx[2][3] = {{0, 0, 0}, {0, 0, 0}};
@@ -620,7 +693,13 @@ __global__ void __launch_bounds__(kThreads, 1)
                 ptx::tmem_wait_ld();
                 if (ch == ch0 + 7) {
                     ptx::tc_fence_before();
-                    ptx::mbar_arrive(&tempty[b]);
+                    if constexpr (PAIR) {
+                        // One arrival per warp, on the even CTA's barrier.
+                        __syncwarp();
+                        if (lane == 0) ptx::mbar_arrive_cluster(ptx::mapa(&tempty[b], 0));
+                    } else {
+                        ptx::mbar_arrive(&tempty[b]);
+                    }
                 }
 #pragma unroll
                 for (int s = 0; s < 4; ++s)
@@ -717,11 +796,19 @@ __global__ void __launch_bounds__(kThreads, 1)
             tk.store(P.S.lists + (size_t)blockIdx.x * P.S.k, P.S.counts + blockIdx.x, bar);
         }
     }
+    // Neither CTA of a pair may release TMEM or leave while the pair's MMAs
+    // can still read its shared memory or write its accumulators.
     ptx::tc_fence_before();
-    __syncthreads();
+    if constexpr (PAIR)
+        ptx::cluster_sync();
+    else
+        __syncthreads();
     if (warp == 1) {
         ptx::tc_fence_after();
-        ptx::tmem_dealloc(tmem, 512);
+        if constexpr (PAIR)
+            ptx::tmem_dealloc_pair(tmem, 512);
+        else
+            ptx::tmem_dealloc(tmem, 512);
     }
 }
 
@@ -744,10 +831,11 @@ static episdet_status get_encoder() {
 }
 
 // rows x pitch bytes, row-major, 128x128-byte boxes, 128-byte swizzle.
-static episdet_status make_tmap(CUtensorMap* m, void* base, uint64_t rows, uint64_t pitch) {
+static episdet_status make_tmap(CUtensorMap* m, void* base, uint64_t rows, uint64_t pitch,
+                                uint32_t box_rows = kTileRows) {
     cuuint64_t dims[2] = {pitch, rows};
     cuuint64_t strides[1] = {pitch};
-    cuuint32_t box[2] = {kKB, kTileRows};
+    cuuint32_t box[2] = {kKB, box_rows};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, base, dims, strides, box, estr,
                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -757,7 +845,10 @@ static episdet_status make_tmap(CUtensorMap* m, void* base, uint64_t rows, uint6
 }
 
 episdet_status tensor_init_attributes() {
-    CUDA_TRY(cudaFuncSetAttribute(tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemTotal));
+    CUDA_TRY(cudaFuncSetAttribute(tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)Cfg<false>::kSmemTotal));
+    CUDA_TRY(cudaFuncSetAttribute(tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)Cfg<true>::kSmemTotal));
     return get_encoder();
 }
 
@@ -817,7 +908,7 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
         p.ntiles = (int)tiles.size();
         p.mode = kPairsScore;
         CUDA_TRY(timer_begin(w));
-        tc_kernel<<<grid, kThreads, kSmemTotal, w->st>>>(tm2, p);
+        tc_kernel<false><<<grid, kThreads, Cfg<false>::kSmemTotal, w->st>>>(tm2, p);
         CHECK_LAUNCH();
         CUDA_TRY(timer_end(w));
         ++*launches;
@@ -834,20 +925,24 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     std::vector<int2> ptiles;
     for (int a = fb / kTileSnps; a < nt; ++a)
         for (int b = a; b < nt; ++b) ptiles.push_back(make_int2(a, b));
-    // Triplet tile lists, one per first row tile t0 = tile(X+1): every (A, B)
-    // tile pair with t0 <= A <= B, ordered in bands of kBand x kBand tiles so
-    // that a wave of concurrent tiles shares few A and B row panels in L2.
-    const int t_first = (fb + 1) / kTileSnps;
+    // Triplet tile lists of the CTA-pair kernel, one per first A pair tile
+    // a0 = (X+1) / 128: every (A pair tile a of 128 SNPs, B tile b of 64 SNPs)
+    // with a0 <= a and 2a <= b, ordered in bands of 768 x 768 SNPs so that a
+    // wave of concurrent tiles shares few A and B row panels in L2.
+    const int nt2 = (M + 2 * kTileSnps - 1) / (2 * kTileSnps);
+    const int a_first = (fb + 1) / (2 * kTileSnps);
+    constexpr int kBandA = kBand / 2;
     std::vector<int2> lists;
-    std::vector<size_t> list_off((size_t)nt + 1, 0);
-    for (int t0 = t_first; t0 < nt; ++t0) {
-        list_off[t0] = lists.size();
-        const int T = nt - t0, nb = (T + kBand - 1) / kBand;
-        for (int ba = 0; ba < nb; ++ba)
-            for (int bb = ba; bb < nb; ++bb)
-                for (int a = ba * kBand; a < std::min(T, (ba + 1) * kBand); ++a)
-                    for (int b = std::max(a, bb * kBand); b < std::min(T, (bb + 1) * kBand); ++b)
-                        lists.push_back(make_int2(t0 + a, t0 + b));
+    std::vector<size_t> list_off((size_t)nt2 + 1, 0);
+    std::vector<int> list_len((size_t)nt2 + 1, 0);
+    for (int a0 = a_first; a0 < nt2; ++a0) {
+        list_off[a0] = lists.size();
+        for (int ba = a0; ba < nt2; ba += kBandA)
+            for (int bb = 2 * ba; bb < nt; bb += kBand)
+                for (int a = ba; a < std::min(nt2, ba + kBandA); ++a)
+                    for (int b = std::max(2 * a, bb); b < std::min(nt, bb + kBand); ++b)
+                        lists.push_back(make_int2(a, b));
+        list_len[a0] = (int)(lists.size() - list_off[a0]);
     }
     CUDA_TRY(w->tiles.ensure(sizeof(int2) * (ptiles.size() + lists.size())));
     int2* d_ptiles = (int2*)w->tiles.p;
@@ -861,7 +956,7 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     p.mode = kPairsStore;
     p.pair_out0 = (uint4*)w->pair4[0].p;
     p.pair_out1 = (uint4*)w->pair4[1].p;
-    tc_kernel<<<grid, kThreads, kSmemTotal, w->st>>>(tm2, p);
+    tc_kernel<false><<<grid, kThreads, Cfg<false>::kSmemTotal, w->st>>>(tm2, p);
     CHECK_LAUNCH();
     ++*launches;
 
@@ -884,21 +979,40 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     for (int i = 0; i < kMaxGroup; ++i) {
         st = make_tmap(&tmx.m[i], w->xsub[i].p, (uint64_t)rows, (uint64_t)pitchx);
         if (st != EPISDET_OK) return st;
+        st = make_tmap(&tmx.m[kMaxGroup + i], w->xsub[i].p, (uint64_t)rows, (uint64_t)pitchx, kTileRows / 2);
+        if (st != EPISDET_OK) return st;
         d_info[i] = (XInfo*)(xw.base + i * xw.stride);
         co.out[i] = (uint8_t*)w->xsub[i].p;
         co.row0[i] = 0;
     }
-    std::vector<int> off((size_t)nt + 1, 0);
-    for (int t = 0; t < nt; ++t) off[t + 1] = off[t] + (nt - t);
     const int xend = std::min(fe, M - 2);
     p.mode = kTriplets;
+    // CTA pairs: as many clusters of two as can be resident at once.
+    int pairs = 0;
+    {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 2;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(2 * (grid / 2), 1, 1);
+        cfg.blockDim = dim3(kThreads, 1, 1);
+        cfg.dynamicSmemBytes = Cfg<true>::kSmemTotal;
+        cfg.stream = w->st;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CUDA_TRY(cudaOccupancyMaxActiveClusters(&pairs, tc_kernel<true>, &cfg));
+        pairs = std::min(pairs, grid / 2);
+        if (pairs < 1) return set_error(EPISDET_ERR_UNSUPPORTED, "no CTA pair of the counting kernel fits on the device");
+    }
     for (int x0 = fb; x0 < xend; x0 += kMaxGroup) {
         const int gn = std::min(kMaxGroup, xend - x0);
         // Index lists and regrouped rows of the gn first SNPs, one launch each.
         xw.x0 = x0;
         xinfo_kernel<<<dim3(2, gn), 1024, 0, w->st>>>(D, xw);
         CHECK_LAUNCH();
-        for (int g = 0; g < gn; ++g) co.row0[g] = 2 * ((x0 + g + 1) / kTileSnps) * kTileSnps;
+        for (int g = 0; g < gn; ++g) co.row0[g] = 2 * ((x0 + g + 1) / (2 * kTileSnps)) * (2 * kTileSnps);
         const int max_rows = rows - co.row0[0];  // the first member needs the most rows
         const dim3 cgrid(cmp_chunks(D.W[0]) + cmp_chunks(D.W[1]), (max_rows + kCmpRows - 1) / kCmpRows, gn);
         compact_kernel<<<cgrid, kCmpThreads, 0, w->st>>>(D, xw, co, rows, pitchx);
@@ -908,20 +1022,34 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
         for (int g = 0; g < gn; ++g) {
             const int x = x0 + g;
             if (progress && x % 256 == 0) printf("Outer loop iteration %d out of %d\n", x / 256, bs_lines);
-            const int t0 = (x + 1) / kTileSnps;
-            p.grp[g] = GroupDesc{d_lists + list_off[t0], cum, x, d_info[g]};
-            cum += off[nt] - off[t0];
+            const int a0 = (x + 1) / (2 * kTileSnps);
+            p.grp[g] = GroupDesc{d_lists + list_off[a0], cum, x, d_info[g]};
+            cum += list_len[a0];
         }
         p.ngroup = gn;
         p.ntiles = cum;
         CUDA_TRY(timer_begin(w));
-        tc_kernel<<<grid, kThreads, kSmemTotal, w->st>>>(tmx, p);
+        {
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = 2;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.gridDim = dim3(2 * pairs, 1, 1);
+            cfg.blockDim = dim3(kThreads, 1, 1);
+            cfg.dynamicSmemBytes = Cfg<true>::kSmemTotal;
+            cfg.stream = w->st;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            CUDA_TRY(cudaLaunchKernelEx(&cfg, tc_kernel<true>, tmx, p));
+        }
         CHECK_LAUNCH();
         CUDA_TRY(timer_end(w));
         *launches += 1;
     }
     if (w->timing) {
-        // Tensor MACs issued: per X, tiles x 128 x 128 x the regrouped K extent,
+        // Tensor MACs issued: per X, pair tiles x 256 x 128 x the regrouped K extent,
         // which follows from X's genotype counts exactly as xinfo_kernel derives it.
         std::vector<int> mg[2];
         for (int c = 0; c < 2; ++c) {
@@ -941,8 +1069,8 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
             for (int c = 0; c < 2; ++c)
                 for (int g = 0; g < 3; ++g)
                     if (g != gd) kext += ((mg[c][(size_t)g * M + x] + kKB - 1) / kKB) * (long)kKB;
-            const int t0 = (x + 1) / kTileSnps;
-            macs += (double)(off[nt] - off[t0]) * kTileRows * kTileRows * (double)kext;
+            const int a0 = (x + 1) / (2 * kTileSnps);
+            macs += (double)list_len[a0] * 2 * kTileRows * kTileRows * (double)kext;
         }
         w->executed_macs = macs;
     }
