@@ -220,6 +220,29 @@ __device__ __forceinline__ void mma_u8_pair(uint32_t d_tmem, uint64_t adesc, uin
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
         : "memory");
 }
+// Pair MMA of packed e2m1 operands with block scales read from TMEM at sfa /
+// sfb (kind::mxf4, 32-value blocks), FP32 accumulate; K = 64 values per MMA.
+__device__ __forceinline__ void mma_mxf4_pair(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                              uint32_t sfa, uint32_t sfb, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::mxf4.block_scale.block32 [%0], %1, %2, %3, [%5], [%6], p;\n\t}" ::"r"(
+            d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(sfa), "r"(sfb)
+        : "memory");
+}
+// Instruction descriptor, kind::mxf4: A/B packed e2m1, K-major, UE8M0 scales, dense K = 64.
+__host__ __device__ constexpr uint32_t idesc_mxf4(uint32_t n, uint32_t m) {
+    return (1u << 7) | (1u << 10) | ((n >> 3) << 17) | (1u << 23) | ((m >> 4) << 24);
+}
+// 32 lanes x 8 consecutive columns, every one set to v.
+__device__ __forceinline__ void tmem_st8_fill(uint32_t taddr, uint32_t v) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(taddr), "r"(v)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
 // Arrives once on the mbarrier at `bar`'s offset in every CTA of cta_mask when
 // all pair MMAs issued so far by this thread complete.
 __device__ __forceinline__ void mma_commit_pair_mc(uint64_t* bar, uint16_t cta_mask) {

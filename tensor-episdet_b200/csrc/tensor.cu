@@ -44,8 +44,16 @@ namespace tc {
 
 constexpr int kTileSnps = 64;
 constexpr int kTileRows = 128;
-constexpr int kKB = 128;  // bytes (samples) per K block
+constexpr int kKB = 128;  // bytes per K block: 128 byte samples (pairs), 256 packed e2m1 samples (triplets)
 constexpr int kTileBytes = kTileRows * kKB;  // one 128-row operand tile of one K block
+// Triplet operands are packed e2m1 (1.0 for a set bit, 0 otherwise), two
+// samples per byte, multiplied by kind::mxf4 with unit block scales.
+constexpr int kF4PerKB = 2 * kKB;  // samples per triplet K block
+constexpr int kZSnpsPair = 56;      // B SNPs per triplet tile (N = 112 rows)
+constexpr int kNPair = 2 * kZSnpsPair;
+// Packed samples per class region of a regrouped row: two segments padded to
+// whole K blocks need at most n + 2 * (kF4PerKB - 1) <= Kc + kClassPad.
+constexpr int kClassPad = 2 * kF4PerKB;
 constexpr int kCap = 2048;  // k <= kMaxTopK kept plus one step of offers
 // Warp 0 issues TMA, warp 1 MMAs; warps 2..9 are the epilogue, two per TMEM
 // lane quarter (warp % 4), each taking half of the 128 accumulator columns in
@@ -56,7 +64,10 @@ constexpr int kEpiPerStep = kEpiThreads * 2;
 static_assert(kMaxTopK + kEpiPerStep <= kCap, "candidate buffer too small for one step of offers");
 constexpr uint64_t kWaitLimitNs = 4000000000ull;
 constexpr uint32_t kIdesc = ptx::idesc_u8(128);
-constexpr uint32_t kIdescPair = ptx::idesc_u8(128, 256);  // CTA-pair MMA, M = 256
+constexpr uint32_t kIdescPair = ptx::idesc_mxf4(kNPair, 256);  // CTA-pair e2m1 MMA, M = 256, N = 112
+// TMEM of the pair kernel: four 112-column count segments, then the block
+// scale factors (every byte 1.0 = UE8M0 127) in columns kSfCol .. 511.
+constexpr uint32_t kSfCol = 4 * kNPair;
 
 enum Mode { kPairsScore = 0, kPairsStore = 1, kTriplets = 2 };
 
@@ -105,12 +116,15 @@ struct TcParams {
 };
 
 // Shared-memory layout of tc_kernel<PAIR>.  A stage holds one K block of this
-// CTA's 128 A rows and of its B rows: all 128 for one CTA, 64 for a CTA pair
-// (PAIR), where the other CTA of the pair holds the other 64.
+// CTA's 128 A rows and of its B rows: all 128 for one CTA, 56 of the pair's
+// 112 for a CTA pair (PAIR), where the other CTA of the pair holds the rest.
 template <bool PAIR>
 struct Cfg {
     static constexpr int kStages = PAIR ? 5 : 4;
-    static constexpr int kBRows = PAIR ? 64 : 128;
+    static constexpr int kBRows = PAIR ? kZSnpsPair : 128;
+    static constexpr int kNSeg = PAIR ? kNPair : 128;      // accumulator columns per count segment
+    static constexpr int kZSnps = PAIR ? kZSnpsPair : kTileSnps;  // B SNPs per tile
+    static constexpr int kChunks = kNSeg / 16;              // 8-column chunks per epilogue warp
     static constexpr int kStageBytes = kTileBytes + kBRows * kKB;
     static constexpr size_t kSmemTopk = (size_t)kStages * kStageBytes;
     static constexpr size_t kSmemLo = kSmemTopk + (size_t)kCap * sizeof(Cand);  // [kLoTab] float
@@ -225,7 +239,8 @@ __global__ void __launch_bounds__(1024) xinfo_kernel(DevData D, XWork xw) {
     const uint32_t* p1 = p0 + W;
     const int per = (W + blockDim.x - 1) / blockDim.x;
     const int w0 = threadIdx.x * per, w1 = min(W, w0 + per);
-    const int base_kb = c == 0 ? 0 : (D.W[0] * 32 + 256) / kKB;
+    // Class 1's region starts after class 0's Kc + kClassPad packed samples.
+    const int base_kb = c == 0 ? 0 : (D.W[0] * 32 + kClassPad) / kF4PerKB;
     int kb = base_kb;
     for (int s = 0; s < 2; ++s) {
         const int g = s == 0 ? ga : gb;
@@ -253,9 +268,9 @@ __global__ void __launch_bounds__(1024) xinfo_kernel(DevData D, XWork xw) {
         if (threadIdx.x == 0) {
             info->len[c][s] = len;
             info->seg[c * 2 + s].kb0 = kb;
-            info->seg[c * 2 + s].kb1 = kb + (len + kKB - 1) / kKB;
+            info->seg[c * 2 + s].kb1 = kb + (len + kF4PerKB - 1) / kF4PerKB;
         }
-        kb += (len + kKB - 1) / kKB;
+        kb += (len + kF4PerKB - 1) / kF4PerKB;
         __syncthreads();
     }
     if (c == 0 && threadIdx.x == 0) {
@@ -266,13 +281,15 @@ __global__ void __launch_bounds__(1024) xinfo_kernel(DevData D, XWork xw) {
     }
 }
 
-// Regrouped operand rows for one X: row r, class c, segment s holds byte
-// bit(r, idx[c][s][k]) at column seg.kb0*128 + k (zero past the segment's
-// length up to its 128-byte end).  Rows below row0 are not needed by X.
+// Regrouped operand rows for one X: row r, class c, segment s holds the e2m1
+// value bit(r, idx[c][s][k]) (1.0 = nibble 2, 0.0 = nibble 0) at packed sample
+// position seg.kb0*256 + k, two samples per byte, the even one in the low
+// nibble (zero past the segment's length up to its 256-sample end).  Rows
+// below row0 are not needed by X.
 //
-// Output-stationary: a CTA owns 4096 output bytes of one class region (the two
-// segments back to back) for kCmpRows rows.  Each thread keeps the source
-// sample indices of its 16 output bytes in registers and reuses them for every
+// Output-stationary: a CTA owns 4096 output samples of one class region (the
+// two segments back to back) for kCmpRows rows.  Each thread keeps the source
+// sample indices of its 16 output samples (8 bytes) in registers and reuses them for every
 // row.  The source words those samples fall in (one contiguous span per row)
 // are copied into a ring of kCmpDepth shared-memory buffers with cp.async,
 // kCmpDepth - 1 rows ahead of the row being gathered, so the copies of later
@@ -284,7 +301,7 @@ constexpr int kCmpRows = 32;
 constexpr int kCmpSpanWords = 2048;
 constexpr int kCmpDepth = 4;
 
-__host__ __device__ inline int cmp_chunks(int words) { return (words * 32 + 256 + kCmpOut - 1) / kCmpOut; }
+__host__ __device__ inline int cmp_chunks(int words) { return (words * 32 + kClassPad + kCmpOut - 1) / kCmpOut; }
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(ptx::smem_u32(dst)), "l"(src) : "memory");
@@ -317,7 +334,7 @@ __global__ void __launch_bounds__(kCmpThreads, 4)
     const int c = (int)blockIdx.x < C0 ? 0 : 1;
     const int chunk = (int)blockIdx.x - (c ? C0 : 0);
     const int la = info->len[c][0], lb = info->len[c][1];
-    const int pa = ((la + kKB - 1) / kKB) * kKB, pb = ((lb + kKB - 1) / kKB) * kKB;
+    const int pa = ((la + kF4PerKB - 1) / kF4PerKB) * kF4PerKB, pb = ((lb + kF4PerKB - 1) / kF4PerKB) * kF4PerKB;
     const int region = pa + pb;
     const int k0 = chunk * kCmpOut;
     if (k0 >= region) return;  // uniform over the CTA
@@ -357,7 +374,7 @@ __global__ void __launch_bounds__(kCmpThreads, 4)
     const int wlo = s_lo & ~3;
     const int nq = s_hi >= s_lo ? (s_hi - wlo + 4) >> 2 : 0;  // 16-byte groups
     const bool staged = nq > 0 && nq * 4 <= kCmpSpanWords;
-    const int colbase = (c ? D.W[0] * 32 + 256 : 0) + kk0;
+    const int colbase = ((c ? D.W[0] * 32 + kClassPad : 0) + kk0) / 2;  // byte of this thread's first sample
     const int rbeg = row0 + (int)blockIdx.y * kCmpRows;
     const int rend = min(row0 + nrows, rbeg + kCmpRows);
     const uint32_t* base = D.bits[c];
@@ -377,27 +394,25 @@ __global__ void __launch_bounds__(kCmpThreads, 4)
             __syncthreads();                 // everyone's have, and the previous row's buffer is free
             issue(row + kCmpDepth - 1);
             const uint32_t* sw = s_src[(row - rbeg) % kCmpDepth];
-            uint32_t o[4] = {0, 0, 0, 0};
+            uint32_t o[2] = {0, 0};
 #pragma unroll
             for (int e = 0; e < 16; ++e) {
                 const int s = src[e];
-                if (s >= 0) o[e >> 2] |= ((sw[(s >> 5) - wlo] >> (31 - (s & 31))) & 1u) << (8 * (e & 3));
+                if (s >= 0) o[e >> 3] |= ((sw[(s >> 5) - wlo] >> (31 - (s & 31))) & 1u) << (4 * (e & 7) + 1);
             }
-            if (kk0 < region)
-                *reinterpret_cast<uint4*>(out + (size_t)row * pitch + colbase) = make_uint4(o[0], o[1], o[2], o[3]);
+            if (kk0 < region) *reinterpret_cast<uint2*>(out + (size_t)row * pitch + colbase) = make_uint2(o[0], o[1]);
         }
         cp_async_wait<0>();
     } else {
         for (int row = rbeg; row < rend; ++row) {
             const uint32_t* srow = base + (size_t)row * W;
-            uint32_t o[4] = {0, 0, 0, 0};
+            uint32_t o[2] = {0, 0};
 #pragma unroll
             for (int e = 0; e < 16; ++e) {
                 const int s = src[e];
-                if (s >= 0) o[e >> 2] |= ((__ldg(srow + (s >> 5)) >> (31 - (s & 31))) & 1u) << (8 * (e & 3));
+                if (s >= 0) o[e >> 3] |= ((__ldg(srow + (s >> 5)) >> (31 - (s & 31))) & 1u) << (4 * (e & 7) + 1);
             }
-            if (kk0 < region)
-                *reinterpret_cast<uint4*>(out + (size_t)row * pitch + colbase) = make_uint4(o[0], o[1], o[2], o[3]);
+            if (kk0 < region) *reinterpret_cast<uint2*>(out + (size_t)row * pitch + colbase) = make_uint2(o[0], o[1]);
         }
     }
 }
@@ -498,6 +513,19 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int rank = PAIR ? (int)ptx::cluster_ctarank() : 0;
     const int t_first = PAIR ? (int)ptx::cluster_id_x() : (int)blockIdx.x;
     const int t_step = PAIR ? (int)ptx::nclusters_x() : (int)gridDim.x;
+    if constexpr (PAIR) {
+        // Block scale factors of every pair MMA: 1.0 in each byte of columns
+        // kSfCol .. 511 of this CTA's TMEM, written before any MMA is issued.
+        if (warp >= 2) {
+            const uint32_t sf = tmem + ((uint32_t)((warp & 3) * 32) << 16) + kSfCol + (uint32_t)(((warp - 2) >> 2) * 32);
+#pragma unroll
+            for (int c = 0; c < 32; c += 8) ptx::tmem_st8_fill(sf + (uint32_t)c, 0x7F7F7F7Fu);
+            ptx::tmem_wait_st();
+        }
+        ptx::tc_fence_before();
+        ptx::cluster_sync();
+        ptx::tc_fence_after();
+    }
 
     if (warp == 0) {
         // ---------------------------------------------------- TMA producer
@@ -521,7 +549,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 const CUtensorMap* tmap = &tm.m[g];
                 const CUtensorMap* tmapb = PAIR ? &tm.m[kMaxGroup + g] : tmap;
                 const int arow0 = PAIR ? tl.x * 2 * kTileRows + rank * kTileRows : tl.x * kTileRows;
-                const int brow0 = PAIR ? tl.y * kTileRows + rank * C::kBRows : tl.y * kTileRows;
+                const int brow0 = PAIR ? tl.y * kNPair + rank * C::kBRows : tl.y * kTileRows;
                 for (int s = 0; ok && s < nseg; ++s)
                     for (int kb = seg[s].kb0; kb < seg[s].kb1; ++kb) {
                         if (!ptx::mbar_wait(&empty[stage], phase ^ 1, abort, kWaitLimitNs)) {
@@ -596,7 +624,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                         for (int kk = 0; kk < kKB / 32; ++kk) {
                             const uint32_t acc = (kb > seg[s].kb0 || kk > 0) ? 1u : 0u;
                             if constexpr (PAIR)
-                                ptx::mma_u8_pair(dbase + (uint32_t)(s * 128), ad + 2 * kk, bd + 2 * kk, kIdescPair, acc);
+                                ptx::mma_mxf4_pair(dbase + (uint32_t)(s * C::kNSeg), ad + 2 * kk, bd + 2 * kk,
+                                                   kIdescPair, tmem + kSfCol, tmem + kSfCol + 32, acc);
                             else
                                 ptx::mma_u8(dbase + (uint32_t)(s * 128), ad + 2 * kk, bd + 2 * kk, kIdesc, acc);
                         }
@@ -632,7 +661,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         // ---------------------------------------------------- epilogue
         const int etid = threadIdx.x - 64;
         const int q = warp & 3;  // TMEM lane quarter this warp may access
-        const int ch0 = ((warp - 2) >> 2) * 8;  // first of this warp's eight 8-column chunks
+        const int ch0 = ((warp - 2) >> 2) * C::kChunks;  // first of this warp's 8-column chunks
         const int m = q * 32 + lane;
         const int yl = m >> 1, j_own = m & 1;
         const int zoff = j_own ? 2 : 0;
@@ -684,14 +713,14 @@ __global__ void __launch_bounds__(kThreads, 1)
                     }
                 }
             }
-            for (int ch = ch0; ch < ch0 + 8; ++ch) {
+            for (int ch = ch0; ch < ch0 + C::kChunks; ++ch) {
                 uint32_t v[4][8];
                 __syncwarp();
 #pragma unroll
                 for (int s = 0; s < 4; ++s)
-                    if (s < nseg) ptx::tmem_ld8(trow + (uint32_t)(s * 128 + ch * 8), v[s]);
+                    if (s < nseg) ptx::tmem_ld8(trow + (uint32_t)(s * C::kNSeg + ch * 8), v[s]);
                 ptx::tmem_wait_ld();
-                if (ch == ch0 + 7) {
+                if (ch == ch0 + C::kChunks - 1) {
                     ptx::tc_fence_before();
                     if constexpr (PAIR) {
                         // One arrival per warp, on the even CTA's barrier.
@@ -716,11 +745,13 @@ __global__ void __launch_bounds__(kThreads, 1)
                 Cand thr = *s_thr;
 #pragma unroll
                 for (int z = 0; z < 2; ++z) {
-                    const int bsnp = tl.y * kTileSnps + ch * 4 + zoff + z;
+                    const int bsnp = tl.y * C::kZSnps + ch * 4 + zoff + z;
                     // cnt(s, jj, kk): A plane jj, B plane kk, segment s
                     auto cnt = [&](int s, int jj, int kk) -> int {
                         const uint32_t own = j_own ? v[s][4 + 2 * z + kk] : v[s][2 * z + kk];
-                        return (int)(jj == j_own ? own : r[s][2 * z + kk]);
+                        const uint32_t raw = jj == j_own ? own : r[s][2 * z + kk];
+                        // Pair counts accumulate in FP32, exact below 2^24.
+                        return PAIR ? (int)__uint_as_float(raw) : (int)raw;
                     };
                     if (mode == kPairsStore) {
                         if (row_ok && arow < bsnp && bsnp < M) {
@@ -926,21 +957,24 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     for (int a = fb / kTileSnps; a < nt; ++a)
         for (int b = a; b < nt; ++b) ptiles.push_back(make_int2(a, b));
     // Triplet tile lists of the CTA-pair kernel, one per first A pair tile
-    // a0 = (X+1) / 128: every (A pair tile a of 128 SNPs, B tile b of 64 SNPs)
-    // with a0 <= a and 2a <= b, ordered in bands of 768 x 768 SNPs so that a
-    // wave of concurrent tiles shares few A and B row panels in L2.
+    // a0 = (X+1) / 128: every (A pair tile a of 128 SNPs, B tile b of 56 SNPs)
+    // with a0 <= a whose Z range reaches past the tile's first Y
+    // (b >= bfirst(a)), ordered in bands of about 768 x 784 SNPs so that a wave
+    // of concurrent tiles shares few A and B row panels in L2.
     const int nt2 = (M + 2 * kTileSnps - 1) / (2 * kTileSnps);
+    const int ntb = (M + kZSnpsPair - 1) / kZSnpsPair;
     const int a_first = (fb + 1) / (2 * kTileSnps);
-    constexpr int kBandA = kBand / 2;
+    constexpr int kBandA = kBand / 2, kBandB = 14;
+    auto bfirst = [](int a) { return (2 * kTileSnps * a) / kZSnpsPair; };
     std::vector<int2> lists;
     std::vector<size_t> list_off((size_t)nt2 + 1, 0);
     std::vector<int> list_len((size_t)nt2 + 1, 0);
     for (int a0 = a_first; a0 < nt2; ++a0) {
         list_off[a0] = lists.size();
         for (int ba = a0; ba < nt2; ba += kBandA)
-            for (int bb = 2 * ba; bb < nt; bb += kBand)
+            for (int bb = bfirst(ba); bb < ntb; bb += kBandB)
                 for (int a = ba; a < std::min(nt2, ba + kBandA); ++a)
-                    for (int b = std::max(2 * a, bb); b < std::min(nt, bb + kBand); ++b)
+                    for (int b = std::max(bfirst(a), bb); b < std::min(ntb, bb + kBandB); ++b)
                         lists.push_back(make_int2(a, b));
         list_len[a0] = (int)(lists.size() - list_off[a0]);
     }
@@ -961,7 +995,8 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     ++*launches;
 
     // Regrouped operands of the kMaxGroup X values of a launch, and their segment tables.
-    const int pitchx = Kc + 256 + Kn + 256;
+    // Regrouped rows: both classes' packed e2m1 regions, 2 samples per byte.
+    const int pitchx = (Kc + kClassPad) / 2 + (Kn + kClassPad) / 2;
     const int max_n = std::max(D.n[0], D.n[1]);
     for (int i = 0; i < kMaxGroup; ++i) CUDA_TRY(w->xsub[i].ensure((size_t)rows * pitchx));
     const size_t info_bytes = 256;
@@ -979,7 +1014,7 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     for (int i = 0; i < kMaxGroup; ++i) {
         st = make_tmap(&tmx.m[i], w->xsub[i].p, (uint64_t)rows, (uint64_t)pitchx);
         if (st != EPISDET_OK) return st;
-        st = make_tmap(&tmx.m[kMaxGroup + i], w->xsub[i].p, (uint64_t)rows, (uint64_t)pitchx, kTileRows / 2);
+        st = make_tmap(&tmx.m[kMaxGroup + i], w->xsub[i].p, (uint64_t)rows, (uint64_t)pitchx, kZSnpsPair);
         if (st != EPISDET_OK) return st;
         d_info[i] = (XInfo*)(xw.base + i * xw.stride);
         co.out[i] = (uint8_t*)w->xsub[i].p;
@@ -1012,7 +1047,7 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
         xw.x0 = x0;
         xinfo_kernel<<<dim3(2, gn), 1024, 0, w->st>>>(D, xw);
         CHECK_LAUNCH();
-        for (int g = 0; g < gn; ++g) co.row0[g] = 2 * ((x0 + g + 1) / (2 * kTileSnps)) * (2 * kTileSnps);
+        for (int g = 0; g < gn; ++g) co.row0[g] = kNPair * bfirst((x0 + g + 1) / (2 * kTileSnps));
         const int max_rows = rows - co.row0[0];  // the first member needs the most rows
         const dim3 cgrid(cmp_chunks(D.W[0]) + cmp_chunks(D.W[1]), (max_rows + kCmpRows - 1) / kCmpRows, gn);
         compact_kernel<<<cgrid, kCmpThreads, 0, w->st>>>(D, xw, co, rows, pitchx);
@@ -1049,7 +1084,7 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
         *launches += 1;
     }
     if (w->timing) {
-        // Tensor MACs issued: per X, pair tiles x 256 x 128 x the regrouped K extent,
+        // Tensor MACs issued: per X, pair tiles x 256 x 112 x the regrouped K extent,
         // which follows from X's genotype counts exactly as xinfo_kernel derives it.
         std::vector<int> mg[2];
         for (int c = 0; c < 2; ++c) {
@@ -1068,9 +1103,9 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
             long kext = 0;
             for (int c = 0; c < 2; ++c)
                 for (int g = 0; g < 3; ++g)
-                    if (g != gd) kext += ((mg[c][(size_t)g * M + x] + kKB - 1) / kKB) * (long)kKB;
+                    if (g != gd) kext += ((mg[c][(size_t)g * M + x] + kF4PerKB - 1) / kF4PerKB) * (long)kF4PerKB;
             const int a0 = (x + 1) / (2 * kTileSnps);
-            macs += (double)list_len[a0] * 2 * kTileRows * kTileRows * (double)kext;
+            macs += (double)list_len[a0] * 2 * kTileRows * kNPair * (double)kext;
         }
         w->executed_macs = macs;
     }
