@@ -28,11 +28,16 @@ def main():
     ap.add_argument("--first-begin", type=int, default=0)
     ap.add_argument("--first-end", type=int, default=0)
     ap.add_argument("--top-k", type=int, default=1024)
-    ap.add_argument("--seed", type=int, default=0xE917)
+    ap.add_argument("--seed", type=lambda v: int(v, 0), default=0xE917)
     ap.add_argument("--maf", type=float, nargs=2, default=(0.05, 0.5))
     ap.add_argument("--repeat", type=int, default=1)
+    ap.add_argument("--planted", default="", help="comma-separated SNP indices of one planted set, e.g. 137,2048,3901")
+    ap.add_argument("--base-risk", type=float, default=0.5)
+    ap.add_argument("--effect", type=float, default=0.25)
     a = ap.parse_args()
-    cases, controls = episdet.generate(a.seed, a.snps, a.cases, a.controls, maf=tuple(a.maf))
+    planted = [tuple(int(v) for v in a.planted.split(","))] if a.planted else []
+    cases, controls = episdet.generate(a.seed, a.snps, a.cases, a.controls, maf=tuple(a.maf), planted=planted,
+                                       base_risk=a.base_risk, effect=a.effect)
     for i in range(a.repeat):
         r = episdet.search(cases, controls, a.cases, a.controls, order=a.order, score=a.score, top_k=a.top_k,
                            engine=a.engine, first_begin=a.first_begin, first_end=a.first_end,
