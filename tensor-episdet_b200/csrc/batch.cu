@@ -2,12 +2,26 @@
 //
 // Neither has a counterpart in hiperbio/tensor-episdet, which searches one
 // dataset with one label vector per process (src/tensor-episdet.cu:159-172).
+//
+// Cohorts of a batch run concurrently: kMaxLanes host workers, each with its
+// own workspace (buffers and stream) on the device, take cohorts in order of
+// decreasing work (C(M, k) x N) from a shared counter and run the ordinary
+// search on them.  Kernels are sized to their work, so the small launches of
+// one cohort (tails of the triplet launch sequence, the single-block
+// candidate merge, small tile sets) leave SMs to the launches of the others.
+// Every cohort's result is computed exactly as by a plain call.
 // A permutation is applied on the GPU: a label vector splits the cohort's
 // sample columns into case and control plane sets in the reference layout,
 // which then go through the ordinary search with device-resident inputs.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <numeric>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "episdet.h"
@@ -62,14 +76,58 @@ extern "C" episdet_status episdet_search_batched(const episdet_dataset* cohorts,
         if (os[i].device != os[0].device)
             return set_error(EPISDET_ERR_INVALID_ARGUMENT, "all cohorts of a batch run on one device");
     }
-    Workspace* w = nullptr;
-    episdet_status st = get_workspace(os[0].device, &w);
-    if (st != EPISDET_OK) return st;
-    std::lock_guard<std::mutex> lock(w->mu);
-    for (int32_t i = 0; i < count; ++i) {
-        st = search_locked(w, &cohorts[i], os[i], &results[i]);
-        if (st != EPISDET_OK) return with_prefix(st, "cohort", i);
+    const int device = os[0].device;
+    const int lanes = std::min<int>(count, kMaxLanes);
+    std::vector<Workspace*> ws((size_t)lanes, nullptr);
+    for (int l = 0; l < lanes; ++l) {
+        episdet_status st = get_workspace_lane(device, l, &ws[(size_t)l]);
+        if (st != EPISDET_OK) return st;
     }
+    // Largest first, so the long cohorts start early and the short ones fill in.
+    std::vector<double> work((size_t)count);
+    for (int32_t i = 0; i < count; ++i) {
+        double m = cohorts[i].num_snps, sets = os[i].order == 2 ? m * (m - 1) / 2 : m * (m - 1) * (m - 2) / 6;
+        work[(size_t)i] = sets * ((double)cohorts[i].num_cases + cohorts[i].num_controls);
+    }
+    std::vector<int32_t> order((size_t)count);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return work[(size_t)a] > work[(size_t)b]; });
+    std::atomic<int32_t> next{0};
+    std::atomic<bool> stop{false};
+    std::mutex fail_mu;
+    episdet_status fail_st = EPISDET_OK;
+    int32_t fail_i = -1;
+    std::string fail_msg;
+    auto worker = [&](int lane) {
+        Workspace* w = ws[(size_t)lane];
+        std::lock_guard<std::mutex> lock(w->mu);
+        if (cudaSetDevice(device) != cudaSuccess) {
+            cudaGetLastError();
+            std::lock_guard<std::mutex> g(fail_mu);
+            if (fail_i < 0) fail_st = EPISDET_ERR_CUDA, fail_i = 0, fail_msg = "cudaSetDevice failed in a batch worker";
+            stop = true;
+            return;
+        }
+        for (;;) {
+            if (stop.load()) return;
+            const int32_t j = next.fetch_add(1);
+            if (j >= count) return;
+            const int32_t i = order[(size_t)j];
+            clear_error();
+            episdet_status st = search_locked(w, &cohorts[i], os[(size_t)i], &results[i]);
+            if (st != EPISDET_OK) {
+                std::lock_guard<std::mutex> g(fail_mu);
+                if (fail_i < 0 || i < fail_i) fail_st = st, fail_i = i, fail_msg = episdet_last_error();
+                stop = true;
+                return;
+            }
+        }
+    };
+    std::vector<std::thread> threads;
+    for (int l = 1; l < lanes; ++l) threads.emplace_back(worker, l);
+    worker(0);
+    for (auto& t : threads) t.join();
+    if (fail_i >= 0) return set_error(fail_st, "cohort %d: %s", fail_i, fail_msg.c_str());
     return EPISDET_OK;
 }
 

@@ -58,9 +58,14 @@ void DevBuf::release() {
 }
 
 static std::mutex g_ws_mu;
-static Workspace* g_ws[64] = {};
+static Workspace* g_ws[64][kMaxLanes] = {};
 
-episdet_status get_workspace(int device, Workspace** out) {
+// Lane 0 serves every single-dataset call; lanes 1.. let the batched entry
+// point run several cohorts at once, each with its own buffers and stream.
+episdet_status get_workspace(int device, Workspace** out) { return get_workspace_lane(device, 0, out); }
+
+episdet_status get_workspace_lane(int device, int lane, Workspace** out) {
+    if (lane < 0 || lane >= kMaxLanes) return set_error(EPISDET_ERR_INVALID_ARGUMENT, "workspace lane %d out of range", lane);
     if (device < 0 || device >= 64) return set_error(EPISDET_ERR_INVALID_ARGUMENT, "device %d out of range", device);
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
@@ -70,7 +75,7 @@ episdet_status get_workspace(int device, Workspace** out) {
     }
     if (device >= ndev) return set_error(EPISDET_ERR_NO_DEVICE, "device %d not present (%d devices)", device, ndev);
     std::lock_guard<std::mutex> g(g_ws_mu);
-    if (!g_ws[device]) {
+    if (!g_ws[device][lane]) {
         CUDA_TRY(cudaSetDevice(device));
         cudaDeviceProp prop;
         CUDA_TRY(cudaGetDeviceProperties(&prop, device));
@@ -90,9 +95,9 @@ episdet_status get_workspace(int device, Workspace** out) {
         CUDA_TRY(cudaFuncSetAttribute(merge_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMergeSmem));
         episdet_status st = tensor_init_attributes();
         if (st != EPISDET_OK) return st;
-        g_ws[device] = w;
+        g_ws[device][lane] = w;
     }
-    *out = g_ws[device];
+    *out = g_ws[device][lane];
     return EPISDET_OK;
 }
 
@@ -528,10 +533,12 @@ extern "C" int32_t episdet_abi_version(void) { return EPISDET_ABI_VERSION; }
 extern "C" episdet_status episdet_release_workspace(int32_t device) {
     if (device < 0 || device >= 64) return set_error(EPISDET_ERR_INVALID_ARGUMENT, "device out of range");
     std::lock_guard<std::mutex> g(g_ws_mu);
-    Workspace* w = g_ws[device];
-    if (!w) return EPISDET_OK;
-    std::lock_guard<std::mutex> l(w->mu);
-    cudaSetDevice(device);
-    w->release_all();
+    for (int lane = 0; lane < kMaxLanes; ++lane) {
+        Workspace* w = g_ws[device][lane];
+        if (!w) continue;
+        std::lock_guard<std::mutex> l(w->mu);
+        cudaSetDevice(device);
+        w->release_all();
+    }
     return EPISDET_OK;
 }

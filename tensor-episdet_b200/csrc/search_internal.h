@@ -72,7 +72,9 @@ struct Workspace {
     }
 };
 
+constexpr int kMaxLanes = 4;  // concurrent cohorts of one batched call
 episdet_status get_workspace(int device, Workspace** out);
+episdet_status get_workspace_lane(int device, int lane, Workspace** out);
 episdet_status build_tables(Workspace* w, int score, int nc, int nn, ScoreTables* T);
 episdet_status stage_dataset(Workspace* w, const episdet_dataset* d, bool validate, DevData* D, uint64_t* launches);
 episdet_status prepare_slots(Workspace* w, int nslots, int k, Slots* S);

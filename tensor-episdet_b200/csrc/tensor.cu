@@ -939,7 +939,9 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
         p.ntiles = (int)tiles.size();
         p.mode = kPairsScore;
         CUDA_TRY(timer_begin(w));
-        tc_kernel<false><<<grid, kThreads, Cfg<false>::kSmemTotal, w->st>>>(tm2, p);
+        // No more CTAs than tiles: SMs left idle stay free for concurrent work.
+        const int g2 = std::max(1, std::min(grid, (int)tiles.size()));
+        tc_kernel<false><<<g2, kThreads, Cfg<false>::kSmemTotal, w->st>>>(tm2, p);
         CHECK_LAUNCH();
         CUDA_TRY(timer_end(w));
         ++*launches;
@@ -990,7 +992,8 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     p.mode = kPairsStore;
     p.pair_out0 = (uint4*)w->pair4[0].p;
     p.pair_out1 = (uint4*)w->pair4[1].p;
-    tc_kernel<false><<<grid, kThreads, Cfg<false>::kSmemTotal, w->st>>>(tm2, p);
+    tc_kernel<false><<<std::max(1, std::min(grid, (int)ptiles.size())), kThreads, Cfg<false>::kSmemTotal, w->st>>>(tm2,
+                                                                                                               p);
     CHECK_LAUNCH();
     ++*launches;
 
@@ -1071,7 +1074,7 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
             attr[0].val.clusterDim.x = 2;
             attr[0].val.clusterDim.y = 1;
             attr[0].val.clusterDim.z = 1;
-            cfg.gridDim = dim3(2 * pairs, 1, 1);
+            cfg.gridDim = dim3(2 * std::max(1, std::min(pairs, cum)), 1, 1);
             cfg.blockDim = dim3(kThreads, 1, 1);
             cfg.dynamicSmemBytes = Cfg<true>::kSmemTotal;
             cfg.stream = w->st;

@@ -314,16 +314,20 @@ def search_pairs_noalloc(cases, controls, num_cases: int, num_controls: int, *, 
 
 
 def search_batched(cohorts, options) -> list:
-    """cohorts: list of (cases, controls, num_cases, num_controls); options: list of dicts for make_options."""
+    """cohorts: list of (cases, controls, num_cases, num_controls[, num_snps]) (num_snps is needed
+    for flat device tensors); options: list of dicts for make_options.  The cohorts run
+    concurrently; each result equals the one a plain search() call returns."""
     n = len(cohorts)
     ds = (Dataset * n)()
     os_ = (Options * n)()
     rs = (Result * n)()
     keep = []
-    for i, ((c, k, nc, nn), opt) in enumerate(zip(cohorts, options)):
+    for i, (co, opt) in enumerate(zip(cohorts, options)):
+        c, k, nc, nn = co[:4]
+        m = int(co[4]) if len(co) > 4 else int(c.shape[0])
         pc, mc = _ptr(c)
         pn, _ = _ptr(k)
-        ds[i] = Dataset(pc, pn, int(c.shape[0]), nc, nn, mc)
+        ds[i] = Dataset(pc, pn, m, nc, nn, mc)
         os_[i] = make_options(**opt)
         r, bufs = _result_buffers(os_[i].top_k)
         rs[i] = r

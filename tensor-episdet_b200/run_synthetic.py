@@ -31,11 +31,12 @@ def main():
     ap.add_argument("--seed", type=lambda v: int(v, 0), default=0xE917)
     ap.add_argument("--maf", type=float, nargs=2, default=(0.05, 0.5))
     ap.add_argument("--repeat", type=int, default=1)
-    ap.add_argument("--planted", default="", help="comma-separated SNP indices of one planted set, e.g. 137,2048,3901")
+    ap.add_argument("--planted", default="",
+                    help="planted sets, comma-separated SNP indices, sets separated by ';' (e.g. 137,2048,3901)")
     ap.add_argument("--base-risk", type=float, default=0.5)
     ap.add_argument("--effect", type=float, default=0.25)
     a = ap.parse_args()
-    planted = [tuple(int(v) for v in a.planted.split(","))] if a.planted else []
+    planted = [tuple(int(v) for v in ps.split(",")) for ps in a.planted.split(";")] if a.planted else []
     cases, controls = episdet.generate(a.seed, a.snps, a.cases, a.controls, maf=tuple(a.maf), planted=planted,
                                        base_risk=a.base_risk, effect=a.effect)
     for i in range(a.repeat):
@@ -43,11 +44,18 @@ def main():
                            engine=a.engine, first_begin=a.first_begin, first_end=a.first_end,
                            flags=episdet.FLAG_TIMING)
     n = a.cases + a.controls
-    print(json.dumps({"snps": list(r.snps), "score": r.score, "sets": r.sets_evaluated, "device_ms": r.device_ms,
-                      "count_kernel_ms": r.count_kernel_ms, "count_launches": r.count_kernel_launches,
-                      "executed_macs": r.executed_macs, "launches": r.kernel_launches,
-                      "tera_sets_samples_per_s": r.sets_evaluated * n / (r.device_ms * 1e-3) / 1e12}))
-
+    out = {"snps": list(r.snps), "score": r.score, "sets": r.sets_evaluated, "device_ms": r.device_ms,
+           "count_kernel_ms": r.count_kernel_ms, "count_launches": r.count_kernel_launches,
+           "executed_macs": r.executed_macs, "launches": r.kernel_launches,
+           "tera_sets_samples_per_s": r.sets_evaluated * n / (r.device_ms * 1e-3) / 1e12}
+    # FP32 ranking score against the FP64 re-score over the candidate list.
+    f32 = r.top_fp32.astype("float64")
+    err = abs(f32 - r.top_fp64)
+    rel = err / abs(r.top_fp64).clip(min=1e-300)
+    out["fp32_vs_fp64"] = {"candidates": int(len(f32)), "max_abs": float(err.max()) if len(err) else 0.0,
+                           "max_rel": float(rel.max()) if len(rel) else 0.0}
+    out["top5"] = [[[int(v) for v in t], float(f)] for t, f in zip(r.top_snps[:5], r.top_fp64[:5])]
+    print(json.dumps(out))
 
 if __name__ == "__main__":
     main()

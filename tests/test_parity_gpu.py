@@ -153,6 +153,42 @@ def test_batched_equals_plain(episdet):
         assert np.array_equal(p.top_snps, b.top_snps)
 
 
+def test_batched_concurrent_lanes_equal_plain(episdet):
+    """More cohorts than worker lanes, uneven sizes, both orders and scores:
+    every result equals the plain call bit for bit."""
+    rng = np.random.default_rng(12)
+    cohorts, opts = [], []
+    for i in range(12):
+        M = int(rng.integers(20, 140))
+        nc, nn = int(rng.integers(64, 6000)), int(rng.integers(64, 6000))
+        c, k = episdet.generate(2000 + i, M, nc, nn)
+        cohorts.append((c, k, nc, nn))
+        opts.append({"order": 2 + (i % 3 == 0), "score": "mi" if i % 4 == 1 else "k2", "top_k": 48})
+    batched = episdet.search_batched(cohorts, opts)
+    for (c, k, nc, nn), opt, b in zip(cohorts, opts, batched):
+        p = episdet.search(c, k, nc, nn, **opt)
+        assert p.snps == b.snps and p.score == b.score
+        assert np.array_equal(p.top_snps, b.top_snps)
+        assert np.array_equal(p.top_fp32.view(np.uint32), b.top_fp32.view(np.uint32))
+        assert np.array_equal(p.top_fp64, b.top_fp64)
+
+
+def test_batched_reports_the_failing_cohort(episdet):
+    cohorts = []
+    for i in range(6):
+        c, k = episdet.generate(3000 + i, 30, 200, 200)
+        cohorts.append((c, k, 200, 200))
+    bad = cohorts[3][0].copy()
+    bad[2, 1, 7] |= 1  # a padding bit: sample 255 >= 200
+    cohorts[3] = (bad, cohorts[3][1], 200, 200)
+    with pytest.raises(episdet.EpisdetError) as e:
+        episdet.search_batched(cohorts, [{"order": 2, "top_k": 16}] * 6)
+    assert e.value.name == "EPISDET_ERR_INVALID_INPUT"
+    assert "cohort 3" in str(e.value)
+    r = episdet.search(*cohorts[0], order=2, top_k=16)  # the library stays usable
+    assert len(r.snps) == 2
+
+
 @pytest.mark.parametrize("variant,order,score", [("pairs.k2", 2, "k2"), ("triplets.mi", 3, "mi"),
                                                  ("triplets.k2", 3, "k2"), ("pairs.mi", 2, "mi")])
 def test_cli_output(episdet, oracle, tmp_path, variant, order, score):
