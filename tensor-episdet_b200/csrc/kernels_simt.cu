@@ -301,14 +301,113 @@ extern "C" __global__ void __launch_bounds__(kSimtThreads)
 // through an 8192-entry bitonic sort in shared memory.
 constexpr int kMergeCap = 8192;
 constexpr int kMergeThreads = 1024;
+constexpr int kRadixBits = 11;
 
+// In-place ascending bitonic sort of buf[0, n) (n a power of two <= kMergeCap).
+__device__ void merge_sort_smem(Cand* buf, int n) {
+    for (int kk = 2; kk <= n; kk <<= 1)
+        for (int j = kk >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < n; i += kMergeThreads) {
+                int ixj = i ^ j;
+                if (ixj > i) {
+                    Cand a = buf[i], b = buf[ixj];
+                    bool up = (i & kk) == 0;
+                    if (up ? cand_better(b, a) : cand_better(a, b)) {
+                        buf[i] = b;
+                        buf[ixj] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+}
+
+// Exact global top-k of the per-CTA candidate lists, by (key, set).
+//
+// Radix selection first: three 11-bit histogram passes over the keys of every
+// listed candidate find T, the k-th smallest key.  The candidates with key <= T
+// contain the top k; they are gathered and sorted alone.  When ties at T
+// exceed the buffer the kernel falls back to merging the lists chunk by chunk.
 extern "C" __global__ void __launch_bounds__(kMergeThreads) merge_topk_kernel(Slots S, Cand* out, int* out_count) {
     extern __shared__ __align__(16) unsigned char smem[];
     Cand* buf = reinterpret_cast<Cand*>(smem);
-    __shared__ int s_r;
+    int* hist = reinterpret_cast<int*>(smem);  // aliases buf while selecting
+    __shared__ uint32_t s_prefix, s_mask;
+    __shared__ int s_need, s_total, s_n;
     const int k = S.k;
     const long total = (long)S.nslots * k;
+    auto key_at = [&](long idx, uint32_t& key) -> bool {
+        const int s = (int)(idx / k), e = (int)(idx % k);
+        if (e >= S.counts[s]) return false;
+        key = S.lists[idx].key;
+        return true;
+    };
+    if (threadIdx.x == 0) {
+        s_prefix = 0;
+        s_mask = 0;
+        s_need = k;
+        s_total = 0;
+    }
+    __syncthreads();
+    // Number of listed candidates.
+    int mine = 0;
+    for (long idx = threadIdx.x; idx < total; idx += kMergeThreads) {
+        uint32_t key;
+        mine += key_at(idx, key) ? 1 : 0;
+    }
+    atomicAdd(&s_total, mine);
+    __syncthreads();
+    uint32_t thr = 0xFFFFFFFFu;  // keep everything when there are at most k candidates
+    if (s_total > k) {
+        for (int pass = 0; pass < 3; ++pass) {
+            const int shift = pass == 0 ? 21 : (pass == 1 ? 10 : 0);
+            const int bits = pass == 2 ? 10 : kRadixBits;
+            const int nb = 1 << bits;
+            for (int i = threadIdx.x; i < nb; i += kMergeThreads) hist[i] = 0;
+            __syncthreads();
+            const uint32_t prefix = s_prefix, mask = s_mask;
+            for (long idx = threadIdx.x; idx < total; idx += kMergeThreads) {
+                uint32_t key;
+                if (key_at(idx, key) && (key & mask) == prefix) atomicAdd(&hist[(key >> shift) & (nb - 1)], 1);
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                int need = s_need, acc = 0, bin = 0;
+                while (acc + hist[bin] < need) acc += hist[bin++];
+                s_need = need - acc;
+                s_prefix = prefix | ((uint32_t)bin << shift);
+                s_mask = mask | ((uint32_t)(nb - 1) << shift);
+            }
+            __syncthreads();
+        }
+        thr = s_prefix;  // the k-th smallest key
+    }
+    // Gather every candidate with key <= thr.
+    if (threadIdx.x == 0) s_n = 0;
+    __syncthreads();
+    for (long idx = threadIdx.x; idx < total; idx += kMergeThreads) {
+        uint32_t key;
+        if (key_at(idx, key) && key <= thr) {
+            const int slot = atomicAdd(&s_n, 1);
+            if (slot < kMergeCap) buf[slot] = S.lists[idx];
+        }
+    }
+    __syncthreads();
+    const int n = s_n;
+    if (n <= kMergeCap) {
+        int p2 = 1;
+        while (p2 < n) p2 <<= 1;
+        for (int i = n + (int)threadIdx.x; i < p2; i += kMergeThreads) buf[i] = cand_worst();
+        __syncthreads();
+        merge_sort_smem(buf, p2);
+        const int r = n < k ? n : k;
+        for (int i = threadIdx.x; i < k; i += kMergeThreads) out[i] = i < r ? buf[i] : cand_worst();
+        if (threadIdx.x == 0) *out_count = r;
+        return;
+    }
+    // Ties at thr overflow the buffer: merge the lists chunk by chunk.
     const int room = kMergeCap - k;
+    __shared__ int s_r;
     if (threadIdx.x == 0) s_r = 0;
     __syncthreads();
     for (long pos = 0; pos < total; pos += room) {
@@ -324,21 +423,7 @@ extern "C" __global__ void __launch_bounds__(kMergeThreads) merge_topk_kernel(Sl
             buf[i] = c;
         }
         __syncthreads();
-        for (int kk = 2; kk <= kMergeCap; kk <<= 1)
-            for (int j = kk >> 1; j > 0; j >>= 1) {
-                for (int i = threadIdx.x; i < kMergeCap; i += kMergeThreads) {
-                    int ixj = i ^ j;
-                    if (ixj > i) {
-                        Cand a = buf[i], b = buf[ixj];
-                        bool up = (i & kk) == 0;
-                        if (up ? cand_better(b, a) : cand_better(a, b)) {
-                            buf[i] = b;
-                            buf[ixj] = a;
-                        }
-                    }
-                }
-                __syncthreads();
-            }
+        merge_sort_smem(buf, kMergeCap);
         if (threadIdx.x == 0) {
             int m = 0;
             while (m < k && buf[m].key != 0xFFFFFFFFu) ++m;
