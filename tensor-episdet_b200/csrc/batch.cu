@@ -131,6 +131,55 @@ extern "C" episdet_status episdet_search_batched(const episdet_dataset* cohorts,
     return EPISDET_OK;
 }
 
+// One label vector of a permutation batch: split the cohort's sample columns
+// into case and control plane sets on the GPU, then search them.
+static episdet_status perm_one(Workspace* w, const uint32_t* d_planes, int M, int n, int W, const uint32_t* label,
+                               bool label_on_device, const episdet_options& o, episdet_result* result) {
+    std::vector<uint32_t> lab((size_t)W);
+    std::vector<int> idx((size_t)n);
+    if (!label_on_device)
+        memcpy(lab.data(), label, sizeof(uint32_t) * W);
+    else {
+        CUDA_TRY(cudaMemcpyAsync(lab.data(), label, sizeof(uint32_t) * W, cudaMemcpyDeviceToHost, w->st));
+        CUDA_TRY(cudaStreamSynchronize(w->st));
+    }
+    int nc = 0;
+    for (int s = 0; s < n; ++s)
+        if ((lab[s / 32] >> (31 - s % 32)) & 1u) idx[nc++] = s;
+    int nn = nc;
+    for (int s = 0; s < n; ++s)
+        if (!((lab[s / 32] >> (31 - s % 32)) & 1u)) idx[nn++] = s;
+    nn -= nc;
+    if (nc < 1 || nn < 1) return set_error(EPISDET_ERR_INVALID_ARGUMENT, "the label leaves a class empty");
+    const int Wc = episdet_class_words(nc), Wn = episdet_class_words(nn);
+    CUDA_TRY(w->perm_idx.ensure(sizeof(int) * (size_t)n));
+    CUDA_TRY(w->perm_cls[0].ensure(sizeof(uint32_t) * (size_t)M * 2 * Wc));
+    CUDA_TRY(w->perm_cls[1].ensure(sizeof(uint32_t) * (size_t)M * 2 * Wn));
+    CUDA_TRY(cudaMemcpyAsync(w->perm_idx.p, idx.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, w->st));
+    // The host vector must outlive the copy.
+    CUDA_TRY(cudaStreamSynchronize(w->st));
+    long t0 = (long)2 * M * Wc, t1 = (long)2 * M * Wn;
+    gather_columns_kernel<<<(unsigned)((t0 + 255) / 256), 256, 0, w->st>>>(d_planes, 2 * M, W, (const int*)w->perm_idx.p,
+                                                                            nc, Wc, (uint32_t*)w->perm_cls[0].p);
+    CHECK_LAUNCH();
+    gather_columns_kernel<<<(unsigned)((t1 + 255) / 256), 256, 0, w->st>>>(
+        d_planes, 2 * M, W, (const int*)w->perm_idx.p + nc, nn, Wn, (uint32_t*)w->perm_cls[1].p);
+    CHECK_LAUNCH();
+    episdet_dataset d;
+    d.cases = (const uint32_t*)w->perm_cls[0].p;
+    d.controls = (const uint32_t*)w->perm_cls[1].p;
+    d.num_snps = M;
+    d.num_cases = nc;
+    d.num_controls = nn;
+    d.memory = EPISDET_DEVICE;
+    episdet_status st = check_dataset(&d, o.order);
+    if (st == EPISDET_OK) st = search_locked(w, &d, o, result);
+    if (st == EPISDET_OK) result->kernel_launches += 2;
+    return st;
+}
+
+// Label vectors run concurrently on the workspace lanes, like the cohorts of a
+// batch; the cohort's planes are read by every lane from one device copy.
 extern "C" episdet_status episdet_search_perm(const episdet_cohort* cohort, const uint32_t* labels,
                                               int32_t num_labels, const episdet_options* opts,
                                               episdet_result* results) {
@@ -144,64 +193,62 @@ extern "C" episdet_status episdet_search_perm(const episdet_cohort* cohort, cons
     episdet_options o;
     episdet_status st = check_options(opts, M, &o);
     if (st != EPISDET_OK) return st;
-    Workspace* w = nullptr;
-    st = get_workspace(o.device, &w);
-    if (st != EPISDET_OK) return st;
-    std::lock_guard<std::mutex> lock(w->mu);
-    CUDA_TRY(cudaSetDevice(o.device));
-    begin_call(w, o);
+    const int lanes = std::min<int>(num_labels, kMaxLanes);
+    std::vector<Workspace*> ws((size_t)lanes, nullptr);
+    for (int l = 0; l < lanes; ++l) {
+        st = get_workspace_lane(o.device, l, &ws[(size_t)l]);
+        if (st != EPISDET_OK) return st;
+    }
     const int W = episdet_class_words(n);
     const size_t plane_words = (size_t)M * 2 * W;
     const uint32_t* d_planes = cohort->planes;
+    Workspace* w0 = ws[0];
+    std::unique_lock<std::mutex> lock0(w0->mu);
+    CUDA_TRY(cudaSetDevice(o.device));
     if (cohort->memory == EPISDET_HOST) {
-        CUDA_TRY(w->perm_planes.ensure(sizeof(uint32_t) * plane_words));
-        CUDA_TRY(cudaMemcpyAsync(w->perm_planes.p, cohort->planes, sizeof(uint32_t) * plane_words,
-                                 cudaMemcpyHostToDevice, w->st));
-        d_planes = (const uint32_t*)w->perm_planes.p;
+        CUDA_TRY(w0->perm_planes.ensure(sizeof(uint32_t) * plane_words));
+        CUDA_TRY(cudaMemcpyAsync(w0->perm_planes.p, cohort->planes, sizeof(uint32_t) * plane_words,
+                                 cudaMemcpyHostToDevice, w0->own_st));
+        CUDA_TRY(cudaStreamSynchronize(w0->own_st));
+        d_planes = (const uint32_t*)w0->perm_planes.p;
     }
-    std::vector<uint32_t> lab((size_t)W);
-    std::vector<int> idx((size_t)n);
-    for (int32_t p = 0; p < num_labels; ++p) {
-        if (cohort->memory == EPISDET_HOST)
-            memcpy(lab.data(), labels + (size_t)p * W, sizeof(uint32_t) * W);
-        else {
-            CUDA_TRY(cudaMemcpyAsync(lab.data(), labels + (size_t)p * W, sizeof(uint32_t) * W, cudaMemcpyDeviceToHost,
-                                     w->st));
-            CUDA_TRY(cudaStreamSynchronize(w->st));
+    const bool on_device = cohort->memory == EPISDET_DEVICE;
+    std::atomic<int32_t> next{0};
+    std::atomic<bool> stop{false};
+    std::mutex fail_mu;
+    episdet_status fail_st = EPISDET_OK;
+    int32_t fail_p = -1;
+    std::string fail_msg;
+    auto worker = [&](int lane) {
+        Workspace* w = ws[(size_t)lane];
+        std::unique_lock<std::mutex> lock;
+        if (lane != 0) lock = std::unique_lock<std::mutex>(w->mu);
+        if (cudaSetDevice(o.device) != cudaSuccess) {
+            cudaGetLastError();
+            std::lock_guard<std::mutex> g(fail_mu);
+            if (fail_p < 0) fail_st = EPISDET_ERR_CUDA, fail_p = 0, fail_msg = "cudaSetDevice failed in a worker";
+            stop = true;
+            return;
         }
-        int nc = 0;
-        for (int s = 0; s < n; ++s)
-            if ((lab[s / 32] >> (31 - s % 32)) & 1u) idx[nc++] = s;
-        int nn = nc;
-        for (int s = 0; s < n; ++s)
-            if (!((lab[s / 32] >> (31 - s % 32)) & 1u)) idx[nn++] = s;
-        nn -= nc;
-        if (nc < 1 || nn < 1) return set_error(EPISDET_ERR_INVALID_ARGUMENT, "label %d leaves a class empty", p);
-        const int Wc = episdet_class_words(nc), Wn = episdet_class_words(nn);
-        CUDA_TRY(w->perm_idx.ensure(sizeof(int) * (size_t)n));
-        CUDA_TRY(w->perm_cls[0].ensure(sizeof(uint32_t) * (size_t)M * 2 * Wc));
-        CUDA_TRY(w->perm_cls[1].ensure(sizeof(uint32_t) * (size_t)M * 2 * Wn));
-        CUDA_TRY(cudaMemcpyAsync(w->perm_idx.p, idx.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, w->st));
-        long t0 = (long)2 * M * Wc, t1 = (long)2 * M * Wn;
-        gather_columns_kernel<<<(unsigned)((t0 + 255) / 256), 256, 0, w->st>>>(d_planes, 2 * M, W,
-                                                                                (const int*)w->perm_idx.p, nc, Wc,
-                                                                                (uint32_t*)w->perm_cls[0].p);
-        CHECK_LAUNCH();
-        gather_columns_kernel<<<(unsigned)((t1 + 255) / 256), 256, 0, w->st>>>(d_planes, 2 * M, W,
-                                                                                (const int*)w->perm_idx.p + nc, nn, Wn,
-                                                                                (uint32_t*)w->perm_cls[1].p);
-        CHECK_LAUNCH();
-        episdet_dataset d;
-        d.cases = (const uint32_t*)w->perm_cls[0].p;
-        d.controls = (const uint32_t*)w->perm_cls[1].p;
-        d.num_snps = M;
-        d.num_cases = nc;
-        d.num_controls = nn;
-        d.memory = EPISDET_DEVICE;
-        st = check_dataset(&d, o.order);
-        if (st == EPISDET_OK) st = search_locked(w, &d, o, &results[p]);
-        if (st != EPISDET_OK) return with_prefix(st, "label", p);
-        results[p].kernel_launches += 2;
-    }
+        for (;;) {
+            if (stop.load()) return;
+            const int32_t p = next.fetch_add(1);
+            if (p >= num_labels) return;
+            clear_error();
+            begin_call(w, o);
+            episdet_status s2 = perm_one(w, d_planes, M, n, W, labels + (size_t)p * W, on_device, o, &results[p]);
+            if (s2 != EPISDET_OK) {
+                std::lock_guard<std::mutex> g(fail_mu);
+                if (fail_p < 0 || p < fail_p) fail_st = s2, fail_p = p, fail_msg = episdet_last_error();
+                stop = true;
+                return;
+            }
+        }
+    };
+    std::vector<std::thread> threads;
+    for (int l = 1; l < lanes; ++l) threads.emplace_back(worker, l);
+    worker(0);
+    for (auto& t : threads) t.join();
+    if (fail_p >= 0) return set_error(fail_st, "label %d: %s", fail_p, fail_msg.c_str());
     return EPISDET_OK;
 }

@@ -17,6 +17,27 @@ sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 import episdet  # noqa: E402
 
 
+def perm(a):
+    """Permutation batch: one cohort, a.permutations label vectors, 2-way or 3-way."""
+    import time
+
+    import numpy as np
+
+    n = a.cases + a.controls
+    planes = episdet.generate_cohort(a.seed, a.snps, n, maf=tuple(a.maf))
+    labels = episdet.generate_labels(a.seed + 1, n, a.cases, a.permutations)
+    t0 = time.perf_counter()
+    res = episdet.search_perm(planes, n, labels, order=a.order, score=a.score, top_k=a.top_k)
+    dt = time.perf_counter() - t0
+    best = np.array([r.score for r in res])
+    sets = sum(r.sets_evaluated for r in res)
+    print(json.dumps({"permutations": len(res), "seconds": dt, "device_ms": sum(r.device_ms for r in res),
+                      "sets": sets, "tera_sets_samples_per_s": sets * n / dt / 1e12,
+                      "label0_best": [list(res[0].snps), res[0].score],
+                      "null_best_scores": {"min": float(best[1:].min()), "median": float(np.median(best[1:])),
+                                           "max": float(best[1:].max())} if len(res) > 1 else None}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--snps", type=int, default=1024)
@@ -35,7 +56,13 @@ def main():
                     help="planted sets, comma-separated SNP indices, sets separated by ';' (e.g. 137,2048,3901)")
     ap.add_argument("--base-risk", type=float, default=0.5)
     ap.add_argument("--effect", type=float, default=0.25)
+    ap.add_argument("--permutations", type=int, default=0,
+                    help="search one cohort of cases+controls samples under this many label vectors "
+                         "(label 0 the first half of the samples, the rest seeded permutations)")
     a = ap.parse_args()
+    if a.permutations:
+        perm(a)
+        return
     planted = [tuple(int(v) for v in ps.split(",")) for ps in a.planted.split(";")] if a.planted else []
     cases, controls = episdet.generate(a.seed, a.snps, a.cases, a.controls, maf=tuple(a.maf), planted=planted,
                                        base_risk=a.base_risk, effect=a.effect)
