@@ -149,6 +149,19 @@ void episdet_free_dataset(episdet_dataset* data);
 /* Writes a dataset in the reference's format: descriptor + <stem>.cases.bin + <stem>.controls.bin. */
 episdet_status episdet_write_dataset(const char* descriptor_path, const episdet_dataset* data);
 
+/* Genotype matrix -> the reference's per-class bit planes, on the GPU.  No
+ * counterpart in the reference, which reads pre-binarized .bin files
+ * (README.md:48-50).  genotypes: [num_snps][num_samples] bytes, each 0, 1 or 2;
+ * is_case: [num_samples] bytes, non-zero marks a case.  cases / controls:
+ * [num_snps][2][episdet_class_words(n)] words for the n cases / controls in
+ * sample order (planes of genotypes 0 and 1, MSB first, zero padding).  All
+ * four arrays live in `memory` (EPISDET_HOST arrays pass through the device).
+ * A genotype above 2 returns EPISDET_ERR_INVALID_INPUT; a class left empty
+ * returns EPISDET_ERR_INVALID_ARGUMENT. */
+episdet_status episdet_binarize(const uint8_t* genotypes, int32_t num_snps, int32_t num_samples,
+                                const uint8_t* is_case, uint32_t* cases, uint32_t* controls, int32_t memory,
+                                int32_t device);
+
 /* Seeded synthetic data (Hardy-Weinberg genotypes, optional planted sets).
  * planted: up to 2 sets of `order` SNP indices (flat array, -1 terminated or
  * num_planted sets); penetrance: P(case) = base, or base + effect for each

@@ -51,6 +51,7 @@ struct Workspace {
     DevBuf xinfo;         // per-X segment tables (tensor engine)
     DevBuf tensor_flag;   // device error / progress words of the tensor engine
     DevBuf perm_planes, perm_cls[2], perm_idx;  // phenotype-permutation staging
+    DevBuf bin_geno, bin_idx, bin_out[2];       // genotype-matrix binarizer staging
     // Per-call accounting.
     int64_t h2d = 0, d2h = 0;
     bool timing = false;
@@ -66,7 +67,8 @@ struct Workspace {
         DevBuf* all[] = {&bits[0], &bits[1], &marg[0], &marg[1], &pair4[0], &pair4[1], &t32, &t64, &slots,
                          &counts, &tiles, &merged, &mcount, &fp64, &flag, &planes8, &xsub[0], &xsub[1], &xsub[2], &xsub[3], &xsub[4], &xsub[5],
                          &xsub[6], &xsub[7], &xinfo,
-                         &tensor_flag, &perm_planes, &perm_cls[0], &perm_cls[1], &perm_idx};
+                         &tensor_flag, &perm_planes, &perm_cls[0], &perm_cls[1], &perm_idx,
+                         &bin_geno, &bin_idx, &bin_out[0], &bin_out[1]};
         for (DevBuf* b : all) b->release();
         tab_score = tab_nc = tab_nn = -1;
     }

@@ -43,7 +43,7 @@ EXPORTED = [
     "episdet_search_perm", "episdet_read_dataset", "episdet_free_dataset", "episdet_write_dataset",
     "episdet_generate", "episdet_generate_cohort", "episdet_generate_labels", "episdet_n_choose_k",
     "episdet_status_string", "episdet_last_error", "episdet_abi_version", "episdet_release_workspace",
-    "episdet_search_pairs_noalloc",
+    "episdet_search_pairs_noalloc", "episdet_binarize",
 ]
 
 
@@ -124,6 +124,9 @@ def lib() -> ctypes.CDLL:
     L.episdet_generate_labels.argtypes = [ctypes.c_uint64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                           ctypes.c_void_p]
     L.episdet_generate_labels.restype = ctypes.c_int
+    L.episdet_binarize.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                   ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]
+    L.episdet_binarize.restype = ctypes.c_int
     L.episdet_n_choose_k.argtypes = [ctypes.c_uint32, ctypes.c_uint32]
     L.episdet_n_choose_k.restype = ctypes.c_uint64
     L.episdet_status_string.argtypes = [ctypes.c_int]
@@ -188,6 +191,38 @@ def generate_labels(seed: int, num_samples: int, num_cases: int, num_labels: int
     labels = np.zeros((num_labels, class_words(num_samples)), dtype=np.uint32)
     _check(lib().episdet_generate_labels(seed, num_samples, num_cases, num_labels, labels.ctypes.data))
     return labels
+
+
+def binarize(genotypes, is_case, device: int = 0):
+    """Dense [SNP][sample] genotype matrix (values 0/1/2, uint8) and a per-sample
+    case flag -> (cases, controls, num_cases, num_controls) in the reference's
+    plane format, built on the GPU.  numpy inputs give numpy outputs; CUDA
+    tensors give CUDA tensors (int32 views of the words)."""
+    M, n = int(genotypes.shape[0]), int(genotypes.shape[1])
+    flags = is_case
+    if hasattr(is_case, "is_cuda"):
+        nc = int(is_case.count_nonzero().item())
+    else:
+        flags = np.ascontiguousarray(np.asarray(is_case).astype(np.uint8) != 0).astype(np.uint8)
+        nc = int(flags.sum())
+    nn = n - nc
+    wc, wn = class_words(max(nc, 1)), class_words(max(nn, 1))
+    if hasattr(genotypes, "is_cuda"):
+        import torch
+
+        g = genotypes.contiguous()
+        f = (flags != 0).to(torch.uint8).contiguous()
+        cases = torch.zeros((M * 2 * wc,), dtype=torch.int32, device=g.device)
+        controls = torch.zeros((M * 2 * wn,), dtype=torch.int32, device=g.device)
+        _check(lib().episdet_binarize(g.data_ptr(), M, n, f.data_ptr(), cases.data_ptr(), controls.data_ptr(),
+                                      DEVICE, device))
+        return cases, controls, nc, nn
+    g = np.ascontiguousarray(genotypes, dtype=np.uint8)
+    cases = np.zeros((M, 2, wc), dtype=np.uint32)
+    controls = np.zeros((M, 2, wn), dtype=np.uint32)
+    _check(lib().episdet_binarize(g.ctypes.data, M, n, flags.ctypes.data, cases.ctypes.data, controls.ctypes.data,
+                                  HOST, device))
+    return cases, controls, nc, nn
 
 
 def read_dataset(path: str):

@@ -153,6 +153,46 @@ def test_batched_equals_plain(episdet):
         assert np.array_equal(p.top_snps, b.top_snps)
 
 
+@pytest.mark.parametrize("n", [1, 33, 1024, 1025, 5000])
+def test_binarize_matches_packing(episdet, oracle, n):
+    """Genotype matrix -> planes on the GPU equals packing each class's columns."""
+    rng = np.random.default_rng(n)
+    M = 37
+    g = rng.integers(0, 3, size=(M, n + 1)).astype(np.uint8)
+    flags = rng.random(n + 1) < 0.4
+    flags[0], flags[-1] = True, False  # both classes non-empty
+    cases, controls, nc, nn = episdet.binarize(g, flags)
+    assert (nc, nn) == (int(flags.sum()), int((~flags).sum()))
+    assert np.array_equal(cases, oracle.pack(g[:, flags]))
+    assert np.array_equal(controls, oracle.pack(g[:, ~flags]))
+
+
+def test_binarize_device_and_search(episdet, oracle):
+    import torch
+
+    rng = np.random.default_rng(5)
+    M, n = 48, 3000
+    g = rng.integers(0, 3, size=(M, n)).astype(np.uint8)
+    flags = rng.random(n) < 0.5
+    dc, dn, nc, nn = episdet.binarize(torch.from_numpy(g).cuda(), torch.from_numpy(flags).cuda())
+    hc, hn, _, _ = episdet.binarize(g, flags)
+    assert np.array_equal(dc.cpu().numpy().view(np.uint32), hc.reshape(-1))
+    r = episdet.search(dc, dn, nc, nn, num_snps=M, order=2, top_k=32)
+    o = oracle.search(hc, hn, nc, nn, order=2, top_k=32)
+    assert tuple(r.snps) == tuple(o["best"])
+
+
+def test_binarize_rejects_bad_values(episdet):
+    g = np.zeros((4, 100), dtype=np.uint8)
+    g[2, 50] = 3
+    with pytest.raises(episdet.EpisdetError) as e:
+        episdet.binarize(g, np.arange(100) % 2 == 0)
+    assert e.value.name == "EPISDET_ERR_INVALID_INPUT"
+    with pytest.raises(episdet.EpisdetError) as e:
+        episdet.binarize(np.zeros((4, 100), dtype=np.uint8), np.zeros(100, dtype=bool))
+    assert e.value.name == "EPISDET_ERR_INVALID_ARGUMENT"
+
+
 def test_batched_concurrent_lanes_equal_plain(episdet):
     """More cohorts than worker lanes, uneven sizes, both orders and scores:
     every result equals the plain call bit for bit."""
