@@ -86,6 +86,12 @@ episdet_status get_workspace_lane(int device, int lane, Workspace** out) {
         w->device = device;
         w->sms = prop.multiProcessorCount;
         CUDA_TRY(cudaStreamCreateWithFlags(&w->own_st, cudaStreamNonBlocking));
+        CUDA_TRY(cudaStreamCreateWithFlags(&w->aux_st, cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&w->ev_ready, cudaEventDisableTiming));
+        for (int i = 0; i < 2; ++i) {
+            CUDA_TRY(cudaEventCreateWithFlags(&w->ev_cmp[i], cudaEventDisableTiming));
+            CUDA_TRY(cudaEventCreateWithFlags(&w->ev_tc[i], cudaEventDisableTiming));
+        }
         w->st = w->own_st;
         CUDA_TRY(cudaEventCreate(&w->e0));
         CUDA_TRY(cudaEventCreate(&w->e1));

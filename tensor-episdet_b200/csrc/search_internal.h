@@ -43,6 +43,8 @@ struct Workspace {
     int sms = 0;
     cudaStream_t st = nullptr;      // stream of the current call (own_st or the caller's)
     cudaStream_t own_st = nullptr;  // the library's own stream
+    cudaStream_t aux_st = nullptr;  // operand regrouping, overlapped with the counting launches
+    cudaEvent_t ev_ready = nullptr, ev_cmp[2] = {}, ev_tc[2] = {};  // ordering between st and aux_st
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     std::mutex mu;
     DevBuf bits[2], marg[2], pair4[2], t32, t64, slots, counts, tiles, merged, mcount, fp64, flag;

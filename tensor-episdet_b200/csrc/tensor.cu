@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(256) unpack_kernel(DevData D, uint8_t* __restr
     }
 }
 
-// Block-wide exclusive scan of one int per thread (blockDim.x = 1024).
+// Block-wide exclusive scan of one int per thread (at most 1024 threads).
 __device__ __forceinline__ int block_exclusive_scan(int v, int* s_warp, int* total) {
     int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int x = v;
@@ -218,7 +218,8 @@ struct XWork {
     __device__ __forceinline__ int* idx(int m) const { return reinterpret_cast<int*>(base + m * stride + info_bytes); }
 };
 
-__global__ void __launch_bounds__(1024) xinfo_kernel(DevData D, XWork xw) {
+constexpr int kXinfoThreads = 256;
+__global__ void __launch_bounds__(kXinfoThreads) xinfo_kernel(DevData D, XWork xw) {
     __shared__ int s_warp[32];
     __shared__ int s_total;
     const int c = blockIdx.x;
@@ -295,10 +296,10 @@ __global__ void __launch_bounds__(1024) xinfo_kernel(DevData D, XWork xw) {
 // kCmpDepth - 1 rows ahead of the row being gathered, so the copies of later
 // rows overlap the gathers of earlier ones.  Spans wider than kCmpSpanWords
 // (first SNPs whose kept genotypes are very rare) gather from global memory.
-constexpr int kCmpOut = 4096;
-constexpr int kCmpThreads = 256;
+constexpr int kCmpOut = 2048;
+constexpr int kCmpThreads = 128;
 constexpr int kCmpRows = 32;
-constexpr int kCmpSpanWords = 2048;
+constexpr int kCmpSpanWords = 1024;
 constexpr int kCmpDepth = 4;
 
 __host__ __device__ inline int cmp_chunks(int words) { return (words * 32 + kClassPad + kCmpOut - 1) / kCmpOut; }
@@ -319,7 +320,7 @@ struct CmpOut {
     int row0[kMaxGroup];
 };
 
-__global__ void __launch_bounds__(kCmpThreads, 4)
+__global__ void __launch_bounds__(kCmpThreads, 8)
     compact_kernel(DevData D, XWork xw, CmpOut co, int rows_total, int pitch) {
     __shared__ __align__(16) uint32_t s_src[kCmpDepth][kCmpSpanWords];
     __shared__ int s_lo, s_hi;
@@ -1001,27 +1002,32 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     // Regrouped rows: both classes' packed e2m1 regions, 2 samples per byte.
     const int pitchx = (Kc + kClassPad) / 2 + (Kn + kClassPad) / 2;
     const int max_n = std::max(D.n[0], D.n[1]);
-    for (int i = 0; i < kMaxGroup; ++i) CUDA_TRY(w->xsub[i].ensure((size_t)rows * pitchx));
+    for (int i = 0; i < 2 * kMaxGroup; ++i) CUDA_TRY(w->xsub[i].ensure((size_t)rows * pitchx));
+    // Two sets of regrouped operands and segment tables: the regrouping of
+    // group g + 1 (on aux_st) overlaps the counting launch of group g (on st).
     const size_t info_bytes = 256;
     const size_t idx_bytes = sizeof(int) * 4 * (size_t)max_n;
-    CUDA_TRY(w->xinfo.ensure(kMaxGroup * (info_bytes + idx_bytes)));
-    TmapPack tmx;
-    memset(&tmx, 0, sizeof(tmx));
-    XInfo* d_info[kMaxGroup];
-    XWork xw;
-    xw.base = (uint8_t*)w->xinfo.p;
-    xw.stride = info_bytes + idx_bytes;
-    xw.info_bytes = info_bytes;
-    xw.max_n = max_n;
-    CmpOut co;
-    for (int i = 0; i < kMaxGroup; ++i) {
-        st = make_tmap(&tmx.m[i], w->xsub[i].p, (uint64_t)rows, (uint64_t)pitchx);
-        if (st != EPISDET_OK) return st;
-        st = make_tmap(&tmx.m[kMaxGroup + i], w->xsub[i].p, (uint64_t)rows, (uint64_t)pitchx, kZSnpsPair);
-        if (st != EPISDET_OK) return st;
-        d_info[i] = (XInfo*)(xw.base + i * xw.stride);
-        co.out[i] = (uint8_t*)w->xsub[i].p;
-        co.row0[i] = 0;
+    CUDA_TRY(w->xinfo.ensure(2 * kMaxGroup * (info_bytes + idx_bytes)));
+    TmapPack tmx[2];
+    XInfo* d_info[2][kMaxGroup];
+    XWork xw[2];
+    CmpOut co[2];
+    for (int b = 0; b < 2; ++b) {
+        memset(&tmx[b], 0, sizeof(tmx[b]));
+        xw[b].base = (uint8_t*)w->xinfo.p + (size_t)b * kMaxGroup * (info_bytes + idx_bytes);
+        xw[b].stride = info_bytes + idx_bytes;
+        xw[b].info_bytes = info_bytes;
+        xw[b].max_n = max_n;
+        for (int i = 0; i < kMaxGroup; ++i) {
+            void* buf = w->xsub[b * kMaxGroup + i].p;
+            st = make_tmap(&tmx[b].m[i], buf, (uint64_t)rows, (uint64_t)pitchx);
+            if (st != EPISDET_OK) return st;
+            st = make_tmap(&tmx[b].m[kMaxGroup + i], buf, (uint64_t)rows, (uint64_t)pitchx, kZSnpsPair);
+            if (st != EPISDET_OK) return st;
+            d_info[b][i] = (XInfo*)(xw[b].base + i * xw[b].stride);
+            co[b].out[i] = (uint8_t*)buf;
+            co[b].row0[i] = 0;
+        }
     }
     const int xend = std::min(fe, M - 2);
     p.mode = kTriplets;
@@ -1044,24 +1050,33 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
         pairs = std::min(pairs, grid / 2);
         if (pairs < 1) return set_error(EPISDET_ERR_UNSUPPORTED, "no CTA pair of the counting kernel fits on the device");
     }
-    for (int x0 = fb; x0 < xend; x0 += kMaxGroup) {
+    // The regrouping reads the planes and marginals staged on st.
+    CUDA_TRY(cudaEventRecord(w->ev_ready, w->st));
+    CUDA_TRY(cudaStreamWaitEvent(w->aux_st, w->ev_ready, 0));
+    int gi = 0;
+    for (int x0 = fb; x0 < xend; x0 += kMaxGroup, ++gi) {
         const int gn = std::min(kMaxGroup, xend - x0);
-        // Index lists and regrouped rows of the gn first SNPs, one launch each.
-        xw.x0 = x0;
-        xinfo_kernel<<<dim3(2, gn), 1024, 0, w->st>>>(D, xw);
+        const int b = gi & 1;
+        // Index lists and regrouped rows of the gn first SNPs, one launch each,
+        // into buffer set b once the counting launch that last read it is done.
+        if (gi >= 2) CUDA_TRY(cudaStreamWaitEvent(w->aux_st, w->ev_tc[b], 0));
+        xw[b].x0 = x0;
+        xinfo_kernel<<<dim3(2, gn), kXinfoThreads, 0, w->aux_st>>>(D, xw[b]);
         CHECK_LAUNCH();
-        for (int g = 0; g < gn; ++g) co.row0[g] = kNPair * bfirst((x0 + g + 1) / (2 * kTileSnps));
-        const int max_rows = rows - co.row0[0];  // the first member needs the most rows
+        for (int g = 0; g < gn; ++g) co[b].row0[g] = kNPair * bfirst((x0 + g + 1) / (2 * kTileSnps));
+        const int max_rows = rows - co[b].row0[0];  // the first member needs the most rows
         const dim3 cgrid(cmp_chunks(D.W[0]) + cmp_chunks(D.W[1]), (max_rows + kCmpRows - 1) / kCmpRows, gn);
-        compact_kernel<<<cgrid, kCmpThreads, 0, w->st>>>(D, xw, co, rows, pitchx);
+        compact_kernel<<<cgrid, kCmpThreads, 0, w->aux_st>>>(D, xw[b], co[b], rows, pitchx);
         CHECK_LAUNCH();
+        CUDA_TRY(cudaEventRecord(w->ev_cmp[b], w->aux_st));
+        CUDA_TRY(cudaStreamWaitEvent(w->st, w->ev_cmp[b], 0));
         *launches += 2;
         int cum = 0;
         for (int g = 0; g < gn; ++g) {
             const int x = x0 + g;
             if (progress && x % 256 == 0) printf("Outer loop iteration %d out of %d\n", x / 256, bs_lines);
             const int a0 = (x + 1) / (2 * kTileSnps);
-            p.grp[g] = GroupDesc{d_lists + list_off[a0], cum, x, d_info[g]};
+            p.grp[g] = GroupDesc{d_lists + list_off[a0], cum, x, d_info[b][g]};
             cum += list_len[a0];
         }
         p.ngroup = gn;
@@ -1080,10 +1095,11 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
             cfg.stream = w->st;
             cfg.attrs = attr;
             cfg.numAttrs = 1;
-            CUDA_TRY(cudaLaunchKernelEx(&cfg, tc_kernel<true>, tmx, p));
+            CUDA_TRY(cudaLaunchKernelEx(&cfg, tc_kernel<true>, tmx[b], p));
         }
         CHECK_LAUNCH();
         CUDA_TRY(timer_end(w));
+        CUDA_TRY(cudaEventRecord(w->ev_tc[b], w->st));
         *launches += 1;
     }
     if (w->timing) {
