@@ -288,19 +288,21 @@ __global__ void __launch_bounds__(kXinfoThreads) xinfo_kernel(DevData D, XWork x
 // nibble (zero past the segment's length up to its 256-sample end).  Rows
 // below row0 are not needed by X.
 //
-// Output-stationary: a CTA owns 4096 output samples of one class region (the
-// two segments back to back) for kCmpRows rows.  Each thread keeps the source
-// sample indices of its 16 output samples (8 bytes) in registers and reuses them for every
-// row.  The source words those samples fall in (one contiguous span per row)
-// are copied into a ring of kCmpDepth shared-memory buffers with cp.async,
-// kCmpDepth - 1 rows ahead of the row being gathered, so the copies of later
-// rows overlap the gathers of earlier ones.  Spans wider than kCmpSpanWords
-// (first SNPs whose kept genotypes are very rare) gather from global memory.
+// Output-stationary: a CTA owns kCmpOut output samples of one class region
+// (the two segments back to back) for kCmpRows rows.  Each thread keeps the
+// source sample indices of its 16 output samples (8 bytes) in registers and
+// reuses them for every row.  The source words those samples fall in (one
+// contiguous span per row) are copied into a ring of kCmpDepth shared-memory
+// buffers with cp.async, kCmpDepth - 1 rows ahead of the row being gathered.
+// Spans wider than kCmpSpanWords (first SNPs whose kept genotypes are rare)
+// gather from global memory.  The kernel is small (128 threads, 64 registers,
+// 4 KB of shared memory) so that its CTAs fit on the SMs beside the counting
+// CTAs: it runs on an auxiliary stream while the previous group is counted.
 constexpr int kCmpOut = 2048;
 constexpr int kCmpThreads = 128;
 constexpr int kCmpRows = 32;
-constexpr int kCmpSpanWords = 1024;
-constexpr int kCmpDepth = 4;
+constexpr int kCmpSpanWords = 512;
+constexpr int kCmpDepth = 2;
 
 __host__ __device__ inline int cmp_chunks(int words) { return (words * 32 + kClassPad + kCmpOut - 1) / kCmpOut; }
 
@@ -424,8 +426,12 @@ __device__ __forceinline__ void record_error(int* err, int code) { atomicCAS(err
 // PAIR: launched as clusters of two CTAs that share each M = 256 x N = 128
 // tile (cta_group::2): the even CTA's MMA warp issues for both, each CTA holds
 // the accumulators of its 128 A rows and scores them.  Triplet mode only.
+// The pair kernel is held to 144 registers a thread: its ten warps then leave
+// room on every SM sub-partition for a warp of the regrouping kernels, which
+// run beside it on the auxiliary stream (at 168 registers they could not, and
+// the regrouping of the next group only ran in the gaps between launches).
 template <bool PAIR>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
     tc_kernel(const __grid_constant__ TmapPack tm, const __grid_constant__ TcParams P) {
     using C = Cfg<PAIR>;
     constexpr int kStages = C::kStages;
