@@ -194,15 +194,32 @@ struct LocalTopK {
     int k;
     int tid;
 
-    __device__ void offer(const Cand& c, const Cand& thr_reg) const {
+    // `hi` is this thread's highest slot + 1 since the last compaction.  The
+    // atomic hands slots out in order, so the largest `hi` over the threads is
+    // the buffer's fill; check() reduces it at a barrier.
+    __device__ void offer(const Cand& c, const Cand& thr_reg, int& hi) const {
         if (cand_better(c, thr_reg)) {
             int slot = atomicAdd(count, 1);
             buf[slot] = c;
+            hi = slot + 1;
+        }
+    }
+
+    // Compacts when the buffer holds more than `limit` entries (limit >= k).
+    // The decision is an OR over the threads' own slots taken at the barrier,
+    // so it is exact and the same in every thread even when faster threads
+    // already offer again after the barrier.
+    template <class Bar>
+    __device__ void check(int& hi, int limit, Bar bar) const {
+        if (bar.any(hi > limit)) {
+            compact(bar);
+            hi = 0;
         }
     }
 
     // Bitonic sort of buf[0..CAP) with entries >= n set to worst; requires a
-    // barrier functor covering exactly the NT participating threads.
+    // barrier functor covering exactly the NT participating threads, and every
+    // offer of those threads must be ordered before the call by a barrier.
     template <class Bar>
     __device__ void compact(Bar bar) const {
         int n = *count;
@@ -242,8 +259,11 @@ struct LocalTopK {
         bar();
     }
 
+    // Every thread's last offers must land before the count is read: callers
+    // reach this without a barrier after their final offers.
     template <class Bar>
     __device__ void store(Cand* __restrict__ slot, int* __restrict__ slot_count, Bar bar) const {
+        bar();
         compact(bar);
         int n = *count;
         for (int i = tid; i < n; i += NT) slot[i] = buf[i];
@@ -253,12 +273,26 @@ struct LocalTopK {
 
 struct BarAll {
     __device__ void operator()() const { __syncthreads(); }
+    __device__ bool any(bool q) const { return __syncthreads_or(q) != 0; }
 };
 
 // Named barrier over `n` threads (multiple of 32) of one CTA.
 struct BarNamed {
     int id, n;
     __device__ void operator()() const { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
+    // Barrier that also returns whether any participating thread passed q.
+    __device__ bool any(bool q) const {
+        uint32_t r;
+        asm volatile(
+            "{\n\t.reg .pred p, q;\n\t"
+            "setp.ne.u32 q, %3, 0;\n\t"
+            "bar.red.or.pred p, %1, %2, q;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(r)
+            : "r"(id), "r"(n), "r"((uint32_t)q)
+            : "memory");
+        return r != 0;
+    }
 };
 
 }  // namespace episdet

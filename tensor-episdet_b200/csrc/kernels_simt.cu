@@ -65,6 +65,7 @@ constexpr int kRowStride = kChunk + 1; // padded shared row (bank spread)
 constexpr int kSimtThreads = 256;
 constexpr int kSimtCap = 4096;         // local top-K capacity
 constexpr int kSimtPerStep = kSimtThreads * 4;
+static_assert(kSimtCap - kSimtPerStep >= kMaxTopK, "the fill check needs room for k entries");
 
 __device__ __forceinline__ void simt_load_tile(uint32_t* s, const uint32_t* __restrict__ bits, int W, int M, int snp0,
                                                int chunk) {
@@ -93,6 +94,7 @@ extern "C" __global__ void __launch_bounds__(kSimtThreads)
     Cand* s_thr = reinterpret_cast<Cand*>(s_count + 4);
 
     LocalTopK<kSimtCap, kSimtThreads> tk{tbuf, s_count, s_thr, S.k, (int)threadIdx.x};
+    int hi = 0;  // this thread's highest candidate slot + 1 since the last compaction
     if (!store_pairs) tk.load(S.lists + (size_t)blockIdx.x * S.k, S.counts[blockIdx.x], BarAll());
     const bool maximize = T.score == 1;
     const int ai = threadIdx.x & 15, bi = threadIdx.x >> 4;
@@ -177,12 +179,9 @@ extern "C" __global__ void __launch_bounds__(kSimtThreads)
                 cd.key = score_key(s, maximize);
                 cd.pad = 0;
                 cd.set = set_key2((uint32_t)a, (uint32_t)b);
-                tk.offer(cd, thr);
+                tk.offer(cd, thr, hi);
             }
-        if (!store_pairs) {
-            __syncthreads();
-            if (*s_count > kSimtCap - kSimtPerStep) tk.compact(BarAll());
-        }
+        if (!store_pairs) tk.check(hi, kSimtCap - kSimtPerStep, BarAll());
     }
     if (!store_pairs) tk.store(S.lists + (size_t)blockIdx.x * S.k, S.counts + blockIdx.x, BarAll());
 }
@@ -203,6 +202,7 @@ extern "C" __global__ void __launch_bounds__(kSimtThreads)
     Cand* s_thr = reinterpret_cast<Cand*>(s_count + 4);
 
     LocalTopK<kSimtCap, kSimtThreads> tk{tbuf, s_count, s_thr, S.k, (int)threadIdx.x};
+    int hi = 0;  // this thread's highest candidate slot + 1 since the last compaction
     tk.load(S.lists + (size_t)blockIdx.x * S.k, S.counts[blockIdx.x], BarAll());
     const bool maximize = T.score == 1;
     const int ai = threadIdx.x & 15, bi = threadIdx.x >> 4;
@@ -288,10 +288,9 @@ extern "C" __global__ void __launch_bounds__(kSimtThreads)
                 cd.key = score_key(s, maximize);
                 cd.pad = 0;
                 cd.set = set_key3((uint32_t)xsnp, (uint32_t)ys, (uint32_t)zs);
-                tk.offer(cd, thr);
+                tk.offer(cd, thr, hi);
             }
-        __syncthreads();
-        if (*s_count > kSimtCap - kSimtPerStep) tk.compact(BarAll());
+        tk.check(hi, kSimtCap - kSimtPerStep, BarAll());
     }
     tk.store(S.lists + (size_t)blockIdx.x * S.k, S.counts + blockIdx.x, BarAll());
 }
@@ -463,6 +462,13 @@ extern "C" __global__ void __launch_bounds__(256)
         zs = (uint32_t)(cd.set & 0x1FFFFF);
     }
     const int M = D.M;
+    // A set outside the dataset (a corrupt candidate) reads no planes: its
+    // score is NaN, which the host reports as an internal error.
+    const bool valid = order == 2 ? (xs < ys && ys < (uint32_t)M) : (xs < ys && ys < zs && zs < (uint32_t)M);
+    if (!valid) {
+        if (lane == 0) fp64_out[warp] = __longlong_as_double(0x7FF8000000000000ll);
+        return;
+    }
     int tab[2][27];
 #pragma unroll
     for (int c = 0; c < 2; ++c) {

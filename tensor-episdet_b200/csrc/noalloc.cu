@@ -231,6 +231,8 @@ extern "C" episdet_status episdet_search_pairs_noalloc(const episdet_dataset* da
     CUDA_TRY(cudaMemcpyAsync(&cnt, mcount, sizeof(int), cudaMemcpyDeviceToHost, stream));
     CUDA_TRY(cudaStreamSynchronize(stream));
     if (cnt < 1) return set_error(EPISDET_ERR_INTERNAL, "no candidate survived the search");
+    for (int i = 0; i < cnt; ++i)
+        if (std::isnan(h_fp64[i])) return set_error(EPISDET_ERR_INTERNAL, "candidate %d holds an invalid SNP set", i);
 
     // FP64 optimum, ties to the lowest set.
     const bool maximize = o.score == EPISDET_SCORE_MI;

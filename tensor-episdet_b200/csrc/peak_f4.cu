@@ -125,6 +125,7 @@ __global__ void __launch_bounds__(kThreads, 1) f4_kernel(int iters, int mode, un
             uint32_t v[8];
             ptx::tmem_ld8(lane_base + (uint32_t)c0, v);
             ptx::tmem_wait_ld();
+            ptx::tmem_regs_ready(v);
             for (int e = 0; e < 8; ++e) {
                 const int col = c0 + e;
                 const float want = (row % 3 == 1 && col % 4 != 0) ? want_one : 0.0f;

@@ -355,6 +355,8 @@ static episdet_status finish(Workspace* w, const DevData& D, const ScoreTables& 
     if (dev_err)
         return set_error(EPISDET_ERR_TIMEOUT, "a bounded device wait gave up (code %d); results discarded", dev_err);
     if (cnt < 1) return set_error(EPISDET_ERR_INTERNAL, "no candidate survived the search");
+    for (int i = 0; i < cnt; ++i)
+        if (std::isnan(f64[i])) return set_error(EPISDET_ERR_INTERNAL, "candidate %d holds an invalid SNP set", i);
     const bool maximize = o.score == EPISDET_SCORE_MI;
     int best = 0;
     for (int i = 1; i < cnt; ++i) {

@@ -123,6 +123,17 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
                  : "memory");
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+// tcgen05.ld fills its registers asynchronously: they hold the loaded values
+// only after tcgen05.wait::ld.  The wait itself names no registers, so a
+// register-only use (a shuffle, a select) could be scheduled above it.  Passing
+// the registers through this volatile statement after the wait makes every use
+// depend on it (volatile statements with a memory clobber keep their order).
+__device__ __forceinline__ void tmem_regs_ready(uint32_t (&v)[8]) {
+    asm volatile(""
+                 : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7])
+                 :
+                 : "memory");
+}
 
 // Shared-memory matrix descriptor: K-major operand, 128-byte swizzle, rows of
 // 128 bytes, 8-row groups 1024 bytes apart (SBO), descriptor version 1.

@@ -676,6 +676,10 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
         const bool maximize = P.T.score == 1;
         const int M = P.D.M;
         LocalTopK<kCap, kEpiThreads> tk{tbuf, s_count, s_thr, P.S.k, etid};
+        // The candidate buffer takes at most kEpiPerStep offers per chunk; its
+        // fill is checked after every chunk.  (Checking less often would need
+        // that many more free slots, i.e. a lower fill limit and more sorts.)
+        int hi = 0;  // this thread's highest candidate slot + 1 since the last compaction
         const LutShared lut{s_lo, P.T.t32};
         if (mode != kPairsStore) {
             // Low end of the FP32 table (every index the scorer can read is < N + 2).
@@ -727,6 +731,9 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                 for (int s = 0; s < 4; ++s)
                     if (s < nseg) ptx::tmem_ld8(trow + (uint32_t)(s * C::kNSeg + ch * 8), v[s]);
                 ptx::tmem_wait_ld();
+#pragma unroll
+                for (int s = 0; s < 4; ++s)
+                    if (s < nseg) ptx::tmem_regs_ready(v[s]);
                 if (ch == ch0 + C::kChunks - 1) {
                     ptx::tc_fence_before();
                     if constexpr (PAIR) {
@@ -789,7 +796,7 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                         cd.key = score_key(sc, maximize);
                         cd.pad = 0;
                         cd.set = set_key2((uint32_t)arow, (uint32_t)bsnp);
-                        tk.offer(cd, thr);
+                        tk.offer(cd, thr, hi);
                         continue;
                     }
                     // triplets: X < Y = arow < Z = bsnp
@@ -819,12 +826,9 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                     cd.key = score_key(sc, maximize);
                     cd.pad = 0;
                     cd.set = set_key3((uint32_t)X, (uint32_t)arow, (uint32_t)bsnp);
-                    tk.offer(cd, thr);
+                    tk.offer(cd, thr, hi);
                 }
-                if (mode != kPairsStore) {
-                    bar();
-                    if (*s_count > kCap - kEpiPerStep) tk.compact(bar);
-                }
+                if (mode != kPairsStore) tk.check(hi, kCap - kEpiPerStep, bar);
             }
         }
         if (!ok) {
