@@ -6,13 +6,22 @@
 // (0.0 and 1.0, four bits each) instead of unsigned bytes: half the bytes per
 // sample and twice the MACs per instruction.  The block scale factors are all
 // 1.0 (UE8M0 127), accumulation is FP32, so a count is exact while it stays
-// below 2^24.  This program checks that on the device and measures the rate:
+// below 2^24.  This program checks that on the device and measures the rate,
+// in both instruction forms:
+//
+//  * cta1: tcgen05.mma.cta_group::1, M = 128, one CTA per SM;
+//  * pair: tcgen05.mma.cta_group::2, M = 256 over a cluster of two CTAs (each
+//    CTA holds 128 A rows and N/2 B rows; the even CTA issues), the form of
+//    the triplet engine;
+//
+// each with a commit every 16 MMAs and every 4 MMAs (the engine commits once
+// per 4-MMA pipeline stage).
 //
 //  * check: A row i is all 1.0 when i % 3 == 1, B row j all 1.0 when j % 4 != 0
-//    (every other value 0), so after `chunks` 128-byte K blocks every D[i][j]
-//    must equal 256 * chunks or 0 -- independent of the swizzle and of the
-//    nibble order inside a byte, which A and B share;
-//  * rate: back-to-back M=128 x N x K=64 MMAs on resident tiles.
+//    (every other value 0), so every D[i][j] must equal the K length or 0 --
+//    independent of the swizzle and of the nibble order inside a byte, which A
+//    and B share;
+//  * rate: back-to-back MMAs on resident tiles, at most 64 in flight.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -27,11 +36,11 @@ namespace {
 
 constexpr int kThreads = 128;
 constexpr uint64_t kLimitNs = 2000000000ull;
-constexpr uint32_t kSfCol = 496;  // scale-factor columns 496..511, every byte 127 (1.0)
+constexpr int kInFlight = 64;  // MMAs in flight at most
+constexpr int kMaxRing = 16;   // commit groups in flight (commit_every >= 4)
 
 __device__ int g_err;
 __device__ unsigned long long g_bad;
-
 
 __device__ __forceinline__ void mma_mxf4(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                                          uint32_t sfa, uint32_t sfb, uint32_t accumulate) {
@@ -44,81 +53,120 @@ __device__ __forceinline__ void mma_mxf4(uint32_t d_tmem, uint64_t adesc, uint64
         : "memory");
 }
 
+template <int N, bool PAIR>
+constexpr size_t smem_bytes() {
+    return 1024 + 16384 + (size_t)(PAIR ? N / 2 : N) * 128 + (kMaxRing + 1) * 8 + 16 + 256;
+}
 
-// mode 0: exactness check over `iters` K blocks; mode 1: rate.
-template <int N>
-__global__ void __launch_bounds__(kThreads, 1) f4_kernel(int iters, int mode, unsigned long long* cycles) {
+// `groups` groups of `cper` MMAs, one commit per group.  check != 0: the
+// exactness check (one accumulator, K = 64 * groups * cper values).
+template <int N, bool PAIR>
+__global__ void __launch_bounds__(kThreads, 1)
+    f4_kernel(int groups, int cper, int check, unsigned long long* cycles) {
+    constexpr int kBRows = PAIR ? N / 2 : N;
+    // Scale factors: columns sf0 .. 511 of every lane hold bytes of 127 (2^0);
+    // the pair form uses the engine's columns 448 .. 511.
+    constexpr uint32_t sf0 = PAIR ? 448u : 496u;
+    constexpr uint32_t sfb_off = PAIR ? 32u : 8u;
     extern __shared__ uint8_t raw[];
     uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(raw) + 1023) & ~uintptr_t(1023));
     uint8_t* a = sm;          // 128 rows x 128 bytes
-    uint8_t* b = sm + 16384;  // N rows x 128 bytes
-    uint64_t* bars = reinterpret_cast<uint64_t*>(b + N * 128);  // [0..3] ring, [4] drain
-    uint32_t* s_tmem = reinterpret_cast<uint32_t*>(bars + 8);
+    uint8_t* b = sm + 16384;  // kBRows rows x 128 bytes
+    uint64_t* bars = reinterpret_cast<uint64_t*>(b + kBRows * 128);  // [0, kMaxRing) ring, [kMaxRing] drain
+    uint32_t* s_tmem = reinterpret_cast<uint32_t*>(bars + kMaxRing + 1);
     int* s_abort = reinterpret_cast<int*>(s_tmem + 1);
     int* s_never = s_abort + 1;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int rank = PAIR ? (int)ptx::cluster_ctarank() : 0;
     // Row-constant operands (a byte holds two e2m1 values: 0x22 = two 1.0).
+    // B row j of the pair's N rows is row j - rank * N/2 of CTA `rank`.
     for (int i = threadIdx.x; i < 128 * 128; i += kThreads) a[i] = ((i >> 7) % 3 == 1) ? 0x22 : 0x00;
-    for (int i = threadIdx.x; i < N * 128; i += kThreads) b[i] = ((i >> 7) % 4 != 0) ? 0x22 : 0x00;
+    for (int i = threadIdx.x; i < kBRows * 128; i += kThreads)
+        b[i] = ((rank * kBRows + (i >> 7)) % 4 != 0) ? 0x22 : 0x00;
     if (threadIdx.x == 0) {
-        for (int i = 0; i < 5; ++i) ptx::mbar_init(&bars[i], 1);
+        for (int i = 0; i <= kMaxRing; ++i) ptx::mbar_init(&bars[i], 1);
         *s_abort = 0;
         *s_never = 0;
         ptx::fence_barrier_init();
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     if (warp == 0) {
-        ptx::tmem_alloc(s_tmem, 512);
-        ptx::tmem_relinquish();
+        if constexpr (PAIR) {
+            ptx::tmem_alloc_pair(s_tmem, 512);
+            ptx::tmem_relinquish_pair();
+        } else {
+            ptx::tmem_alloc(s_tmem, 512);
+            ptx::tmem_relinquish();
+        }
     }
     ptx::tc_fence_before();
-    __syncthreads();
+    if constexpr (PAIR)
+        ptx::cluster_sync();
+    else
+        __syncthreads();
     ptx::tc_fence_after();
     const uint32_t tmem = *s_tmem;
-    // Scale factors: every byte of columns kSfCol .. kSfCol + 15 is 127 (2^0).
     const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
-    ptx::tmem_st8_fill(lane_base + kSfCol, 0x7F7F7F7Fu);
-    ptx::tmem_st8_fill(lane_base + kSfCol + 8, 0x7F7F7F7Fu);
+    for (uint32_t c = sf0; c < 512u; c += 8) ptx::tmem_st8_fill(lane_base + c, 0x7F7F7F7Fu);
     ptx::tmem_wait_st();
+    // Both CTAs' operands and scale factors are in place before the first MMA.
     ptx::tc_fence_before();
-    __syncthreads();
+    if constexpr (PAIR)
+        ptx::cluster_sync();
+    else
+        __syncthreads();
     ptx::tc_fence_after();
     volatile int* abort = s_abort;
     if (warp == 0 && lane == 0) {
-        const uint32_t idesc = ptx::idesc_mxf4(N, 128);
-        const uint64_t ad = ptx::smem_desc_sw128(ptx::smem_u32(a)), bd = ptx::smem_desc_sw128(ptx::smem_u32(b));
-        const uint32_t sfa = tmem + kSfCol, sfb = tmem + kSfCol + 8;
-        long long t0 = clock64();
-        uint32_t ph = 0;
-        for (int it = 0; it < iters; ++it) {
-            const int slot = it & 3;
-            if (it >= 4) {  // at most 4 groups of 16 MMAs in flight
-                if (!ptx::mbar_wait(&bars[slot], (ph >> slot) & 1u, abort, kLimitNs)) {
-                    atomicExch(&g_err, 1);
-                    *s_abort = 1;
-                    break;
+        if (rank == 0) {
+            const uint32_t idesc = ptx::idesc_mxf4(N, PAIR ? 256 : 128);
+            const uint64_t ad = ptx::smem_desc_sw128(ptx::smem_u32(a)), bd = ptx::smem_desc_sw128(ptx::smem_u32(b));
+            const uint32_t sfa = tmem + sf0, sfb = tmem + sf0 + sfb_off;
+            const int ring = kInFlight / cper;
+            long long t0 = clock64();
+            uint32_t ph = 0;
+            uint32_t gm = 0;
+            for (int g = 0; g < groups; ++g) {
+                const int slot = g % ring;
+                if (g >= ring) {
+                    if (!ptx::mbar_wait(&bars[slot], (ph >> slot) & 1u, abort, kLimitNs)) {
+                        atomicExch(&g_err, 1);
+                        *s_abort = 1;
+                        break;
+                    }
+                    ph ^= 1u << slot;
                 }
-                ph ^= 1u << slot;
+                for (int m = 0; m < cper; ++m, ++gm) {
+                    const int kk = gm & 3;  // 4 MMAs of K = 64 cover one 128-byte block
+                    // Two accumulator regions below the scale factors (one for N = 256).
+                    const uint32_t acc = (check || N > 224) ? 0u : ((gm >> 2) & 1u) * (uint32_t)N;
+                    const uint32_t first = (check && gm == 0) ? 0u : 1u;
+                    if constexpr (PAIR)
+                        ptx::mma_mxf4_pair(tmem + acc, ad + 2 * kk, bd + 2 * kk, idesc, sfa, sfb, first);
+                    else
+                        mma_mxf4(tmem + acc, ad + 2 * kk, bd + 2 * kk, idesc, sfa, sfb, first);
+                }
+                if constexpr (PAIR)
+                    ptx::mma_commit_pair_mc(&bars[slot], 0x3);  // as the engine: both CTAs' barriers
+                else
+                    ptx::mma_commit(&bars[slot]);
             }
-            for (int m = 0; m < 16; ++m) {
-                const int kk = m & 3;  // 4 MMAs of K = 64 cover one 128-byte block
-                // Two accumulator regions below the scale-factor columns (one for N = 256).
-                const uint32_t acc = (mode == 0 || N > 224) ? 0u : (uint32_t)((m >> 2) & 1) * N;
-                const uint32_t first = (mode == 0 && it == 0 && m == 0) ? 0u : 1u;
-                mma_mxf4(tmem + acc, ad + 2 * kk, bd + 2 * kk, idesc, sfa, sfb, first);
-            }
-            ptx::mma_commit(&bars[slot]);
+            if constexpr (PAIR)
+                ptx::mma_commit_pair_mc(&bars[kMaxRing], 0x3);
+            else
+                ptx::mma_commit(&bars[kMaxRing]);
+            if (!ptx::mbar_wait(&bars[kMaxRing], 0, s_never, kLimitNs)) atomicExch(&g_err, 2);
+            cycles[blockIdx.x] = (unsigned long long)(clock64() - t0);
+        } else if (!ptx::mbar_wait(&bars[kMaxRing], 0, s_never, kLimitNs)) {
+            atomicExch(&g_err, 3);  // the odd CTA: its accumulators are complete
         }
-        ptx::mma_commit(&bars[4]);
-        if (!ptx::mbar_wait(&bars[4], 0, s_never, kLimitNs)) atomicExch(&g_err, 2);
-        cycles[blockIdx.x] = (unsigned long long)(clock64() - t0);
     }
     ptx::tc_fence_before();
     __syncthreads();
     ptx::tc_fence_after();
-    if (mode == 0 && blockIdx.x == 0) {
-        // Each iteration adds 4 K blocks of 128 bytes = 4 x 256 values.
-        const float want_one = 1024.0f * (float)iters;
+    const int unit = PAIR ? (int)ptx::cluster_id_x() : (int)blockIdx.x;
+    if (check && unit == 0) {
+        const float want_one = 64.0f * (float)groups * (float)cper;
         const int row = warp * 32 + lane;
         unsigned long long bad = 0;
         for (int c0 = 0; c0 < N; c0 += 8) {
@@ -134,11 +182,19 @@ __global__ void __launch_bounds__(kThreads, 1) f4_kernel(int iters, int mode, un
         }
         if (bad) atomicAdd(&g_bad, bad);
     }
+    // Neither CTA of a pair releases TMEM or leaves while the pair's MMAs may
+    // still read its shared memory.
     ptx::tc_fence_before();
-    __syncthreads();
+    if constexpr (PAIR)
+        ptx::cluster_sync();
+    else
+        __syncthreads();
     if (warp == 0) {
         ptx::tc_fence_after();
-        ptx::tmem_dealloc(tmem, 512);
+        if constexpr (PAIR)
+            ptx::tmem_dealloc_pair(tmem, 512);
+        else
+            ptx::tmem_dealloc(tmem, 512);
     }
 }
 
@@ -153,14 +209,34 @@ __global__ void __launch_bounds__(kThreads, 1) f4_kernel(int iters, int mode, un
         }                                                                                   \
     } while (0)
 
-template <int N>
-static int run(int sms, int iters, int mode, unsigned long long* d_cyc) {
-    const size_t smem = 1024 + 16384 + N * 128 + 256;
-    CK(cudaFuncSetAttribute(f4_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int grid = mode == 0 ? 1 : sms;
-    if (mode == 1) {
-        f4_kernel<N><<<grid, kThreads, smem>>>(64, mode, d_cyc);  // warm-up
-        CK(cudaGetLastError());
+template <int N, bool PAIR>
+static int launch(int grid, int groups, int cper, int check, unsigned long long* d_cyc) {
+    const size_t smem = smem_bytes<N, PAIR>();
+    CK(cudaFuncSetAttribute(f4_kernel<N, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = PAIR ? 2 : 1;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&cfg, f4_kernel<N, PAIR>, groups, cper, check, d_cyc));
+    CK(cudaGetLastError());
+    return 0;
+}
+
+// check: one CTA (one pair); rate: one CTA per SM.  iters = 16-MMA units.
+template <int N, bool PAIR>
+static int run(int sms, int iters, int cper, int check, unsigned long long* d_cyc) {
+    const int unit = PAIR ? 2 : 1;
+    const int grid = check ? unit : (sms / unit) * unit;
+    const int groups = iters * 16 / cper;
+    if (!check) {
+        if (launch<N, PAIR>(grid, 64 * 16 / cper, cper, 0, d_cyc)) return 1;  // warm-up
         CK(cudaDeviceSynchronize());
     }
     unsigned long long zero = 0;
@@ -169,8 +245,7 @@ static int run(int sms, int iters, int mode, unsigned long long* d_cyc) {
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     CK(cudaEventRecord(e0));
-    f4_kernel<N><<<grid, kThreads, smem>>>(iters, mode, d_cyc);
-    CK(cudaGetLastError());
+    if (launch<N, PAIR>(grid, groups, cper, check, d_cyc)) return 1;
     CK(cudaEventRecord(e1));
     CK(cudaEventSynchronize(e1));
     int err = 0;
@@ -180,15 +255,27 @@ static int run(int sms, int iters, int mode, unsigned long long* d_cyc) {
     CK(cudaMemcpy(&cyc, d_cyc, sizeof(cyc), cudaMemcpyDeviceToHost));
     float ms = 0.0f;
     CK(cudaEventElapsedTime(&ms, e0, e1));
-    const double per_cta = (double)iters * 16.0 * 128.0 * N * 64.0;
-    if (mode == 0)
-        printf("{\"n\": %d, \"mode\": \"check\", \"k_values\": %d, \"bad_cells\": %llu, \"err\": %d}\n", N,
-               iters * 1024, bad, err);
-    else
-        printf("{\"n\": %d, \"mode\": \"rate\", \"ms\": %.3f, \"tmacs_per_s\": %.1f, \"mac_per_clk_per_sm\": %.0f, "
+    CK(cudaEventDestroy(e0));
+    CK(cudaEventDestroy(e1));
+    // MACs of one SM: its 128 rows of D (the pair's M = 256 is split over two SMs).
+    const double per_sm = (double)groups * cper * 128.0 * N * 64.0;
+    const char* form = PAIR ? "pair" : "cta1";
+    if (check)
+        printf("{\"form\": \"%s\", \"n\": %d, \"mode\": \"check\", \"k_values\": %d, \"bad_cells\": %llu, "
                "\"err\": %d}\n",
-               N, ms, per_cta * grid / (ms * 1e-3) / 1e12, per_cta / (double)cyc, err);
+               form, N, groups * cper * 64, bad, err);
+    else
+        printf("{\"form\": \"%s\", \"n\": %d, \"commit_every\": %d, \"mode\": \"rate\", \"ms\": %.3f, "
+               "\"tmacs_per_s\": %.1f, \"mac_per_clk_per_sm\": %.0f, \"err\": %d}\n",
+               form, N, cper, ms, per_sm * grid / (ms * 1e-3) / 1e12, per_sm / (double)cyc, err);
     return err || bad ? 1 : 0;
+}
+
+template <int N, bool PAIR>
+static int rates(int sms, int iters, unsigned long long* d_cyc) {
+    int rc = run<N, PAIR>(sms, iters, 16, 0, d_cyc);
+    rc |= run<N, PAIR>(sms, iters, 4, 0, d_cyc);
+    return rc;
 }
 
 int main(int argc, char** argv) {
@@ -201,17 +288,24 @@ int main(int argc, char** argv) {
         return 1;
     }
     printf("{\"gpu\": \"%s\", \"sms\": %d}\n", p.name, p.multiProcessorCount);
+    const int sms = p.multiProcessorCount;
     unsigned long long* d_cyc = nullptr;
-    CK(cudaMalloc(&d_cyc, sizeof(unsigned long long) * p.multiProcessorCount));
+    CK(cudaMalloc(&d_cyc, sizeof(unsigned long long) * sms));
     int rc = 0;
-    // Exactness first (one CTA; 4096 iterations = 4,194,304 values per count).
-    rc |= run<128>(p.multiProcessorCount, 4096, 0, d_cyc);
-    rc |= run<112>(p.multiProcessorCount, 4096, 0, d_cyc);
-    rc |= run<256>(p.multiProcessorCount, 64, 0, d_cyc);
+    // Exactness first (4096 x 16 MMAs = 4,194,304 values per count).
+    rc |= run<128, false>(sms, 4096, 16, 1, d_cyc);
+    rc |= run<112, false>(sms, 4096, 16, 1, d_cyc);
+    rc |= run<256, false>(sms, 64, 16, 1, d_cyc);
+    rc |= run<112, true>(sms, 4096, 16, 1, d_cyc);
+    rc |= run<128, true>(sms, 4096, 16, 1, d_cyc);
+    rc |= run<256, true>(sms, 64, 16, 1, d_cyc);
     if (rc) return rc;
-    rc |= run<128>(p.multiProcessorCount, iters, 1, d_cyc);
-    rc |= run<112>(p.multiProcessorCount, iters, 1, d_cyc);
-    rc |= run<256>(p.multiProcessorCount, iters, 1, d_cyc);
+    rc |= rates<128, false>(sms, iters, d_cyc);
+    rc |= rates<112, false>(sms, iters, d_cyc);
+    rc |= rates<256, false>(sms, iters, d_cyc);
+    rc |= rates<112, true>(sms, iters, d_cyc);
+    rc |= rates<128, true>(sms, iters, d_cyc);
+    rc |= rates<256, true>(sms, iters, d_cyc);
     CK(cudaFree(d_cyc));
     return rc;
 }

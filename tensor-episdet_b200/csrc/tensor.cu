@@ -75,7 +75,8 @@ struct Seg {
     int kb0, kb1;  // K-block range [kb0, kb1)
 };
 
-// Per-X sample regrouping: genotypes ga < gb of X are kept, gd is derived.
+// Per-X sample regrouping: genotypes ga and gb of X are kept (ga the larger
+// group), gd (the largest) is derived.
 struct XInfo {
     int gd, ga, gb, pad;
     int len[2][2];  // [class][kept genotype] samples
@@ -83,6 +84,8 @@ struct XInfo {
 };
 
 constexpr int kMaxGroup = 4;  // first SNPs (X) per triplet launch
+constexpr int kStageMin = 16384;    // samples of segment 0 from which the staged kernel copies it out
+constexpr int kStageClass = 65536;  // class size from which triplet launches use the staged kernel
 constexpr int kBand = 12;     // tile-band edge of the triplet tile order
 
 // Tensor maps of a launch, one per X (each X has its own regrouped operand
@@ -115,10 +118,10 @@ struct TcParams {
     int* err;
 };
 
-// Shared-memory layout of tc_kernel<PAIR>.  A stage holds one K block of this
+// Shared-memory layout of tc_kernel<PAIR, STAGE>.  A stage holds one K block of this
 // CTA's 128 A rows and of its B rows: all 128 for one CTA, 56 of the pair's
 // 112 for a CTA pair (PAIR), where the other CTA of the pair holds the rest.
-template <bool PAIR>
+template <bool PAIR, bool STAGE = false>
 struct Cfg {
     static constexpr int kStages = PAIR ? 5 : 4;
     static constexpr int kBRows = PAIR ? kZSnpsPair : 128;
@@ -128,7 +131,10 @@ struct Cfg {
     static constexpr int kStageBytes = kTileBytes + kBRows * kKB;
     static constexpr size_t kSmemTopk = (size_t)kStages * kStageBytes;
     static constexpr size_t kSmemLo = kSmemTopk + (size_t)kCap * sizeof(Cand);  // [kLoTab] float
-    static constexpr size_t kSmemBars = kSmemLo + (size_t)kLoTab * sizeof(float);
+    // STAGE: count segment 0 of the tile copied out of TMEM as 16-bit counts,
+    // [epilogue thread][chunk] x 8 columns.
+    static constexpr size_t kSmemStage = kSmemLo + (size_t)kLoTab * sizeof(float);
+    static constexpr size_t kSmemBars = kSmemStage + (STAGE ? (size_t)kEpiThreads * kChunks * sizeof(uint4) : 0);
     static constexpr int kNumBars = 2 * kStages + 5;  // full, empty, tfull[2], tempty[2], drain
     static constexpr size_t kSmemMisc = kSmemBars + ((kNumBars * sizeof(uint64_t) + 63) & ~size_t(63));
     static constexpr size_t kSmemGroup = kSmemMisc + 64;
@@ -141,6 +147,10 @@ struct Cfg {
 struct GroupSm {
     Seg seg[4];
     int ga, gb, x, empty_mask;
+    // Pair kernel: when the counts of segment 0 (cases, X = ga) fit 16 bits,
+    // the epilogue copies that segment out of TMEM first and releases its
+    // columns early, so the next tile's segment-0 MMAs overlap the epilogue.
+    int stage_ok, pad;
 };
 static_assert(sizeof(GroupSm) * kMaxGroup <= 256, "group table size");
 
@@ -234,7 +244,10 @@ __global__ void __launch_bounds__(kXinfoThreads) xinfo_kernel(DevData D, XWork x
     int gd = 0;
     if (tot[1] > tot[gd]) gd = 1;
     if (tot[2] > tot[gd]) gd = 2;
-    const int ga = gd == 0 ? 1 : 0, gb = gd == 2 ? 1 : 2;
+    // Kept genotypes; segment 0 holds the larger group (the pair kernel
+    // copies segment 0 out of TMEM early to overlap the next tile's MMAs).
+    const int o1 = gd == 0 ? 1 : 0, o2 = gd == 2 ? 1 : 2;
+    const int ga = tot[o2] > tot[o1] ? o2 : o1, gb = ga == o1 ? o2 : o1;
     const int W = D.W[c], n = D.n[c];
     const uint32_t* p0 = D.bits[c] + (size_t)X * 2 * W;
     const uint32_t* p1 = p0 + W;
@@ -430,10 +443,11 @@ __device__ __forceinline__ void record_error(int* err, int code) { atomicCAS(err
 // room on every SM sub-partition for a warp of the regrouping kernels, which
 // run beside it on the auxiliary stream (at 168 registers they could not, and
 // the regrouping of the next group only ran in the gaps between launches).
-template <bool PAIR>
+template <bool PAIR, bool STAGE>
 __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
     tc_kernel(const __grid_constant__ TmapPack tm, const __grid_constant__ TcParams P) {
-    using C = Cfg<PAIR>;
+    static_assert(PAIR || !STAGE, "staging is a pair-kernel mode");
+    using C = Cfg<PAIR, STAGE>;
     constexpr int kStages = C::kStages;
     constexpr int kStageBytes = C::kStageBytes;
     extern __shared__ uint8_t smem_raw[];
@@ -453,6 +467,7 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
     int* s_epi_fail = reinterpret_cast<int*>(smem + C::kSmemMisc + 12);
     int* s_count = reinterpret_cast<int*>(smem + C::kSmemMisc + 16);
     Cand* s_thr = reinterpret_cast<Cand*>(smem + C::kSmemMisc + 32);
+    uint4* s_stage = reinterpret_cast<uint4*>(smem + C::kSmemStage);
     volatile int* abort = s_abort;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -478,6 +493,11 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
         gs.empty_mask = 0;
         for (int s = 0; s < 4; ++s)
             if (gs.seg[s].kb1 <= gs.seg[s].kb0) gs.empty_mask |= 1 << s;
+        gs.pad = 0;
+        // A count of the segment is at most its sample count; short segments
+        // are not worth the copy.
+        const int len0 = STAGE && mode == kTriplets ? P.grp[threadIdx.x].xinfo->len[0][0] : 0;
+        gs.stage_ok = len0 >= kStageMin && len0 <= 65535;
         s_grp[threadIdx.x] = gs;
     }
 
@@ -557,7 +577,7 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                 const CUtensorMap* tmapb = PAIR ? &tm.m[kMaxGroup + g] : tmap;
                 const int arow0 = PAIR ? tl.x * 2 * kTileRows + rank * kTileRows : tl.x * kTileRows;
                 const int brow0 = PAIR ? tl.y * kNPair + rank * C::kBRows : tl.y * kTileRows;
-                for (int s = 0; ok && s < nseg; ++s)
+                for (int s = 0; ok && s < nseg; ++s) {
                     for (int kb = seg[s].kb0; kb < seg[s].kb1; ++kb) {
                         if (!ptx::mbar_wait(&empty[stage], phase ^ 1, abort, kWaitLimitNs)) {
                             ok = false;
@@ -582,6 +602,7 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                             phase ^= 1;
                         }
                     }
+                }
             }
             if (!ok) {
                 record_error(P.err, 1);
@@ -606,19 +627,34 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
             bool ok = true;
             int local = 0;
             for (int t = t_first; ok && t < P.ntiles; t += t_step, ++local) {
-                const Seg* seg = s_grp[group_of(P, t)].seg;
+                const GroupSm& gs = s_grp[group_of(P, t)];
+                const Seg* seg = gs.seg;
                 const int b = local % nbuf;
                 const uint32_t use = (uint32_t)(local / nbuf);
-                // Both CTAs' epilogues must have drained accumulator set b.
-                const bool freed = PAIR ? ptx::mbar_wait_cluster(&tempty[b], (use & 1) ^ 1, abort, kWaitLimitNs)
-                                        : ptx::mbar_wait(&tempty[b], (use & 1) ^ 1, abort, kWaitLimitNs);
-                if (!freed) {
-                    ok = false;
-                    break;
+                // Pair kernel: segment 0's columns are free once both CTAs'
+                // epilogues have copied out (or finished with) the previous tile's.
+                if constexpr (STAGE) {
+                    if (!ptx::mbar_wait_cluster(&tempty[1], (use & 1) ^ 1, abort, kWaitLimitNs)) {
+                        ok = false;
+                        break;
+                    }
+                    ptx::tc_fence_after();
                 }
-                ptx::tc_fence_after();
+                // The other segments wait for the whole accumulator set to be
+                // drained by both CTAs' epilogues.
+                const int late_at = (STAGE && gs.stage_ok) ? 1 : 0;
                 const uint32_t dbase = tmem + (uint32_t)(b * nseg * 128);
-                for (int s = 0; ok && s < nseg; ++s)
+                for (int s = 0; ok && s < nseg; ++s) {
+                    if (s == late_at) {
+                        const bool freed = PAIR ? ptx::mbar_wait_cluster(&tempty[0], (use & 1) ^ 1, abort, kWaitLimitNs)
+                                                : ptx::mbar_wait(&tempty[b], (use & 1) ^ 1, abort, kWaitLimitNs);
+                        if (!freed) {
+                            ok = false;
+                            break;
+                        }
+                        ptx::tc_fence_after();
+                    }
+                    const uint32_t dseg = dbase + (uint32_t)(s * C::kNSeg);
                     for (int kb = seg[s].kb0; kb < seg[s].kb1; ++kb) {
                         if (!ptx::mbar_wait(&full[stage], phase, abort, kWaitLimitNs)) {
                             ok = false;
@@ -631,10 +667,10 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                         for (int kk = 0; kk < kKB / 32; ++kk) {
                             const uint32_t acc = (kb > seg[s].kb0 || kk > 0) ? 1u : 0u;
                             if constexpr (PAIR)
-                                ptx::mma_mxf4_pair(dbase + (uint32_t)(s * C::kNSeg), ad + 2 * kk, bd + 2 * kk,
-                                                   kIdescPair, tmem + kSfCol, tmem + kSfCol + 32, acc);
+                                ptx::mma_mxf4_pair(dseg, ad + 2 * kk, bd + 2 * kk, kIdescPair, tmem + kSfCol,
+                                                   tmem + kSfCol + 32, acc);
                             else
-                                ptx::mma_u8(dbase + (uint32_t)(s * 128), ad + 2 * kk, bd + 2 * kk, kIdesc, acc);
+                                ptx::mma_u8(dseg, ad + 2 * kk, bd + 2 * kk, kIdesc, acc);
                         }
                         if constexpr (PAIR)
                             ptx::mma_commit_pair_mc(&empty[stage], 0x3);  // frees the stage in both CTAs
@@ -645,6 +681,7 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                             phase ^= 1;
                         }
                     }
+                }
                 if (ok) {
                     if constexpr (PAIR)
                         ptx::mma_commit_pair_mc(&tfull[b], 0x3);
@@ -705,9 +742,33 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
             }
             ptx::tc_fence_after();
             const int ga = s_grp[g].ga, gb = s_grp[g].gb, emask = s_grp[g].empty_mask;
+            const bool stg = STAGE && s_grp[g].stage_ok;
             // This thread's A SNP (pairs: a, triplets: Y); a pair tile spans 128 A SNPs.
             const int arow = PAIR ? tl.x * 2 * kTileSnps + rank * kTileSnps + yl : tl.x * kTileSnps + yl;
             const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * nseg * 128);
+            if constexpr (STAGE) {
+                if (stg) {
+                    // Copy this thread's columns of segment 0 to shared memory
+                    // as 16-bit counts, then release them to the next tile's
+                    // first MMAs.
+                    for (int ch = ch0; ch < ch0 + C::kChunks; ++ch) {
+                        uint32_t w[8];
+                        __syncwarp();
+                        ptx::tmem_ld8(trow + (uint32_t)(ch * 8), w);
+                        ptx::tmem_wait_ld();
+                        ptx::tmem_regs_ready(w);
+                        uint32_t h[4];
+#pragma unroll
+                        for (int e = 0; e < 4; ++e)
+                            h[e] = (uint32_t)(int)__uint_as_float(w[2 * e]) |
+                                   ((uint32_t)(int)__uint_as_float(w[2 * e + 1]) << 16);
+                        s_stage[etid * C::kChunks + (ch - ch0)] = make_uint4(h[0], h[1], h[2], h[3]);
+                    }
+                    ptx::tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) ptx::mbar_arrive_cluster(ptx::mapa(&tempty[1], 0));
+                }
+            }
             // Per-row constants.
             int ma[2][3] = {{0, 0, 0}, {0, 0, 0}}, mx[2][3] = {{0, 0, 0}, {0, 0, 0}};
             int xy9[2][9];
@@ -729,7 +790,17 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                 __syncwarp();
 #pragma unroll
                 for (int s = 0; s < 4; ++s)
-                    if (s < nseg) ptx::tmem_ld8(trow + (uint32_t)(s * C::kNSeg + ch * 8), v[s]);
+                    if (s < nseg) {
+                        if (s == 0 && stg) {
+                            const uint4 h = s_stage[etid * C::kChunks + (ch - ch0)];
+                            const uint32_t hw[4] = {h.x, h.y, h.z, h.w};
+#pragma unroll
+                            for (int e = 0; e < 8; ++e)
+                                v[s][e] = __float_as_uint((float)((hw[e >> 1] >> (16 * (e & 1))) & 0xFFFFu));
+                        } else {
+                            ptx::tmem_ld8(trow + (uint32_t)(s * C::kNSeg + ch * 8), v[s]);
+                        }
+                    }
                 ptx::tmem_wait_ld();
 #pragma unroll
                 for (int s = 0; s < 4; ++s)
@@ -737,9 +808,13 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                 if (ch == ch0 + C::kChunks - 1) {
                     ptx::tc_fence_before();
                     if constexpr (PAIR) {
-                        // One arrival per warp, on the even CTA's barrier.
+                        // One arrival per warp, on the even CTA's barriers: the
+                        // whole set (b == 0), and segment 0 unless it was staged.
                         __syncwarp();
-                        if (lane == 0) ptx::mbar_arrive_cluster(ptx::mapa(&tempty[b], 0));
+                        if (lane == 0) {
+                            ptx::mbar_arrive_cluster(ptx::mapa(&tempty[b], 0));
+                            if (STAGE && !stg) ptx::mbar_arrive_cluster(ptx::mapa(&tempty[1], 0));
+                        }
                     } else {
                         ptx::mbar_arrive(&tempty[b]);
                     }
@@ -887,10 +962,12 @@ static episdet_status make_tmap(CUtensorMap* m, void* base, uint64_t rows, uint6
 }
 
 episdet_status tensor_init_attributes() {
-    CUDA_TRY(cudaFuncSetAttribute(tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CUDA_TRY(cudaFuncSetAttribute(tc_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)Cfg<false>::kSmemTotal));
-    CUDA_TRY(cudaFuncSetAttribute(tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CUDA_TRY(cudaFuncSetAttribute(tc_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)Cfg<true>::kSmemTotal));
+    CUDA_TRY(cudaFuncSetAttribute(tc_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)Cfg<true, true>::kSmemTotal));
     return get_encoder();
 }
 
@@ -952,7 +1029,7 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
         CUDA_TRY(timer_begin(w));
         // No more CTAs than tiles: SMs left idle stay free for concurrent work.
         const int g2 = std::max(1, std::min(grid, (int)tiles.size()));
-        tc_kernel<false><<<g2, kThreads, Cfg<false>::kSmemTotal, w->st>>>(tm2, p);
+        tc_kernel<false, false><<<g2, kThreads, Cfg<false>::kSmemTotal, w->st>>>(tm2, p);
         CHECK_LAUNCH();
         CUDA_TRY(timer_end(w));
         ++*launches;
@@ -1003,7 +1080,7 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     p.mode = kPairsStore;
     p.pair_out0 = (uint4*)w->pair4[0].p;
     p.pair_out1 = (uint4*)w->pair4[1].p;
-    tc_kernel<false><<<std::max(1, std::min(grid, (int)ptiles.size())), kThreads, Cfg<false>::kSmemTotal, w->st>>>(tm2,
+    tc_kernel<false, false><<<std::max(1, std::min(grid, (int)ptiles.size())), kThreads, Cfg<false>::kSmemTotal, w->st>>>(tm2,
                                                                                                                p);
     CHECK_LAUNCH();
     ++*launches;
@@ -1041,6 +1118,11 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     }
     const int xend = std::min(fe, M - 2);
     p.mode = kTriplets;
+    // Large classes make the staged kernel's early release of segment 0 pay
+    // (its MMAs then overlap the epilogue); smaller ones run the plain kernel.
+    const bool staged = std::min(D.n[0], D.n[1]) >= kStageClass;
+    auto* const kern = staged ? tc_kernel<true, true> : tc_kernel<true, false>;
+    const size_t ksmem = staged ? Cfg<true, true>::kSmemTotal : Cfg<true>::kSmemTotal;
     // CTA pairs: as many clusters of two as can be resident at once.
     int pairs = 0;
     {
@@ -1052,11 +1134,11 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
         attr[0].val.clusterDim.z = 1;
         cfg.gridDim = dim3(2 * (grid / 2), 1, 1);
         cfg.blockDim = dim3(kThreads, 1, 1);
-        cfg.dynamicSmemBytes = Cfg<true>::kSmemTotal;
+        cfg.dynamicSmemBytes = ksmem;
         cfg.stream = w->st;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        CUDA_TRY(cudaOccupancyMaxActiveClusters(&pairs, tc_kernel<true>, &cfg));
+        CUDA_TRY(cudaOccupancyMaxActiveClusters(&pairs, kern, &cfg));
         pairs = std::min(pairs, grid / 2);
         if (pairs < 1) return set_error(EPISDET_ERR_UNSUPPORTED, "no CTA pair of the counting kernel fits on the device");
     }
@@ -1101,11 +1183,11 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
             attr[0].val.clusterDim.z = 1;
             cfg.gridDim = dim3(2 * std::max(1, std::min(pairs, cum)), 1, 1);
             cfg.blockDim = dim3(kThreads, 1, 1);
-            cfg.dynamicSmemBytes = Cfg<true>::kSmemTotal;
+            cfg.dynamicSmemBytes = ksmem;
             cfg.stream = w->st;
             cfg.attrs = attr;
             cfg.numAttrs = 1;
-            CUDA_TRY(cudaLaunchKernelEx(&cfg, tc_kernel<true>, tmx[b], p));
+            CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, tmx[b], p));
         }
         CHECK_LAUNCH();
         CUDA_TRY(timer_end(w));

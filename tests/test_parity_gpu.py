@@ -63,6 +63,20 @@ def test_config1_pairs_k2(episdet, oracle, engine):
     assert_same(r, o, 1024)
 
 
+@pytest.mark.parametrize("score", ["k2", "mi"])
+def test_large_classes_triplets(episdet, oracle, score):
+    """Classes of >= 65,536 samples: the triplet launches use the kernel that
+    copies count segment 0 out of TMEM early; first SNPs whose segment 0 holds
+    fewer than 16,384 samples (low MAF) run it without the copy, so both paths
+    meet in one launch."""
+    cases, controls = episdet.generate(0xE91A, 44, 70000, 66000, maf=(0.02, 0.5))
+    k = 256
+    r = episdet.search(cases, controls, 70000, 66000, order=3, score=score, top_k=k, engine="tensor")
+    o = oracle.search(cases, controls, 70000, 66000, order=3, score=score, top_k=k)
+    assert_same(r, o, k)
+    assert r.sets_evaluated == o["sets"]
+
+
 @pytest.mark.parametrize("engine", ENGINES)
 def test_planted_triplet(episdet, oracle, engine):
     cases, controls = episdet.generate(0xE917, 96, 8192, 8192, planted=[(5, 40, 77)], base_risk=0.5, effect=0.25)
