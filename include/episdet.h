@@ -141,6 +141,42 @@ episdet_status episdet_search_batched(const episdet_dataset* cohorts, const epis
 episdet_status episdet_search_perm(const episdet_cohort* cohort, const uint32_t* labels, int32_t num_labels,
                                    const episdet_options* opts, episdet_result* results);
 
+/* Permutation significance -- no counterpart in the reference, which prints
+ * one best set (src/tensor-episdet.cu:181-185).  results[0] is the search
+ * under the observed labels, results[1..num_labels-1] under permuted ones (as
+ * episdet_search_perm returns them).  Single-step max-statistic adjusted
+ * p-values (Westfall-Young): for a set with FP64 score s,
+ *   p = (1 + #{i >= 1 : results[i].score at least as extreme as s}) / num_labels,
+ * "at least as extreme" meaning <= s for K2 (minimised) and >= s for MI.
+ * pvalues[j] is the p-value of entry j of results[0]'s top list when it has
+ * one (top_count > 0, top_fp64 set), else pvalues[0] is the best set's;
+ * *count receives the number written (at most capacity). */
+episdet_status episdet_perm_pvalues(const episdet_result* results, int32_t num_labels, int32_t score,
+                                    double* pvalues, int32_t capacity, int32_t* count);
+
+/* Resumable search -- a checkpoint cursor for long runs; no counterpart in
+ * the reference.  The first-SNP range of opts is searched in num_slabs slabs
+ * of about equal work (episdet_search with first_begin/first_end); after each
+ * slab the merged top_k candidate list (sets, FP32 and FP64 scores) and the
+ * cursor (next first SNP) are written to `path` (a temporary file renamed
+ * over it, so an interrupted call leaves the previous checkpoint).  A call
+ * that finds a checkpoint of the same search (same sizes, options and plane
+ * contents, by a 64-bit fingerprint) continues from its cursor; one of another
+ * search is refused with EPISDET_ERR_INVALID_ARGUMENT.  Merging the slabs'
+ * top_k lists by (FP32 score, set) gives exactly the list of one uninterrupted
+ * search, so the final result is the same. */
+typedef struct episdet_resume {
+    const char* path;       /* checkpoint file */
+    int32_t num_slabs;      /* slabs over the whole first-SNP range; 0 -> 16 */
+    int32_t max_slabs;      /* > 0: return after this many slabs (done = 0 if work remains) */
+    int32_t done;           /* out: 1 when the search is complete and `result` holds its answer */
+    int32_t next_first;     /* out: the cursor, first SNP of the next slab */
+    int32_t slabs_run;      /* out: slabs searched by this call */
+    int32_t reserved[3];
+} episdet_resume;
+episdet_status episdet_search_resumable(const episdet_dataset* data, const episdet_options* opts,
+                                        episdet_resume* resume, episdet_result* result);
+
 /* Reads the reference's 5-line dataset descriptor and its two .bin files
  * (src/tensor-episdet.cu:58-148) into malloc'd arrays; free with episdet_free_dataset. */
 episdet_status episdet_read_dataset(const char* descriptor_path, episdet_dataset* out);

@@ -43,7 +43,7 @@ EXPORTED = [
     "episdet_search_perm", "episdet_read_dataset", "episdet_free_dataset", "episdet_write_dataset",
     "episdet_generate", "episdet_generate_cohort", "episdet_generate_labels", "episdet_n_choose_k",
     "episdet_status_string", "episdet_last_error", "episdet_abi_version", "episdet_release_workspace",
-    "episdet_search_pairs_noalloc", "episdet_binarize",
+    "episdet_search_pairs_noalloc", "episdet_binarize", "episdet_perm_pvalues", "episdet_search_resumable",
 ]
 
 
@@ -80,6 +80,12 @@ class Result(ctypes.Structure):
                 ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64), ("top_capacity", ctypes.c_int32),
                 ("top_snps", ctypes.POINTER(ctypes.c_uint32)), ("top_fp32", ctypes.POINTER(ctypes.c_float)),
                 ("top_fp64", ctypes.POINTER(ctypes.c_double))]
+
+
+class Resume(ctypes.Structure):
+    _fields_ = [("path", ctypes.c_char_p), ("num_slabs", ctypes.c_int32), ("max_slabs", ctypes.c_int32),
+                ("done", ctypes.c_int32), ("next_first", ctypes.c_int32), ("slabs_run", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 3)]
 
 
 class Synth(ctypes.Structure):
@@ -330,6 +336,45 @@ def search(cases, controls, num_cases: int, num_controls: int, *, num_snps: Opti
     r, bufs = _result_buffers(top_k)
     _check(lib().episdet_search(ctypes.byref(d), ctypes.byref(o), ctypes.byref(r)))
     return _to_result(order, r, bufs)
+
+
+def search_resumable(cases, controls, num_cases: int, num_controls: int, checkpoint: str, *,
+                     num_snps: Optional[int] = None, order: int = 3, score="k2", top_k: int = 1024, device: int = 0,
+                     engine="auto", first_begin: int = 0, first_end: int = 0, flags: int = 0, num_slabs: int = 16,
+                     max_slabs: int = 0):
+    """Search in first-SNP slabs with a checkpoint file after each slab;
+    rerunning with the same arguments continues from the checkpoint.
+    Returns (SearchResult, done, next_first): the answer when done, else the
+    best set and list of the slabs searched so far."""
+    pc, mc = _ptr(cases)
+    pn, mn = _ptr(controls)
+    if mc != mn:
+        raise TypeError("cases and controls must live in the same memory")
+    M = num_snps if num_snps is not None else int(cases.shape[0])
+    d = Dataset(pc, pn, M, num_cases, num_controls, mc)
+    o = make_options(order, score, top_k, device, engine, first_begin, first_end, flags)
+    rs = Resume()
+    rs.path = os.fsencode(checkpoint)
+    rs.num_slabs, rs.max_slabs = num_slabs, max_slabs
+    r, bufs = _result_buffers(top_k)
+    _check(lib().episdet_search_resumable(ctypes.byref(d), ctypes.byref(o), ctypes.byref(rs), ctypes.byref(r)))
+    return _to_result(order, r, bufs), bool(rs.done), int(rs.next_first)
+
+
+def perm_pvalues(results, score="k2") -> np.ndarray:
+    """Single-step max-statistic adjusted p-values of the observed labels'
+    top list (results[0], as search_perm returns it) against the best scores
+    of the permuted labels results[1:]: (1 + #{perm best at least as extreme})
+    / len(results); lower is more extreme for K2, higher for MI.  Same rule as
+    episdet_perm_pvalues."""
+    if len(results) < 2:
+        raise ValueError("need the observed labels and at least one permutation")
+    maximize = (score == "mi") if isinstance(score, str) else int(score) == SCORE_MI
+    obs = results[0]
+    s = obs.top_fp64 if len(obs.top_fp64) else np.array([obs.score])
+    null = np.array([r.score for r in results[1:]])
+    hits = (null[None, :] >= s[:, None]) if maximize else (null[None, :] <= s[:, None])
+    return (1.0 + hits.sum(axis=1)) / len(results)
 
 
 def search_pairs_noalloc(cases, controls, num_cases: int, num_controls: int, *, num_snps: int, score="k2",

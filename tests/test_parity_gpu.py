@@ -4,6 +4,7 @@ Bar: the best set, the FP32 candidate list (sets and FP32 score bits) and the
 FP64 re-scores are identical to the oracle's, because every count is exact
 and both sides evaluate the same score tables with the same operation order.
 """
+import ctypes
 import json
 import os
 import subprocess
@@ -149,6 +150,62 @@ def test_permutations_match_split_searches(episdet, oracle):
         cases, controls, nc, nn = oracle.split_by_label(planes, n, lab)
         o = oracle.search(cases, controls, nc, nn, order=2, score="k2", top_k=64)
         assert_same(r, o, 64)
+
+
+def test_perm_pvalues_of_a_permutation_search(episdet):
+    n, M, nl = 3000, 50, 24
+    planes = episdet.generate_cohort(31, M, n)
+    labels = episdet.generate_labels(32, n, 1400, nl)
+    res = episdet.search_perm(planes, n, labels, order=2, score="k2", top_k=16)
+    pv = episdet.perm_pvalues(res, "k2")
+    null = np.array([r.score for r in res[1:]])
+    assert pv.shape == (16,)
+    for s, p in zip(res[0].top_fp64, pv):
+        assert p == (1 + (null <= s).sum()) / nl
+    # The C entry point over the same scores.
+    rs = (episdet.Result * nl)()
+    top = np.ascontiguousarray(res[0].top_fp64)
+    rs[0].score, rs[0].top_count = res[0].score, len(top)
+    rs[0].top_fp64 = top.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    for i in range(1, nl):
+        rs[i].score = res[i].score
+    out = np.zeros(16)
+    cnt = ctypes.c_int32()
+    assert episdet.lib().episdet_perm_pvalues(rs, nl, episdet.SCORE_K2, out.ctypes.data_as(
+        ctypes.POINTER(ctypes.c_double)), 16, ctypes.byref(cnt)) == 0
+    assert cnt.value == 16 and np.array_equal(out, pv)
+
+
+@pytest.mark.parametrize("order,M,nc,nn,device", [(3, 60, 700, 1300, False), (2, 300, 900, 1100, True),
+                                                  (3, 44, 70000, 66000, False)])
+def test_resumable_equals_one_search(episdet, tmp_path, order, M, nc, nn, device):
+    """A search interrupted after every two slabs and resumed from its
+    checkpoint gives the uninterrupted search's answer bit for bit."""
+    import torch
+    cases, controls = episdet.generate(0xE91B + M, M, nc, nn)
+    k = 128
+    plain = episdet.search(cases, controls, nc, nn, order=order, top_k=k, engine="tensor")
+    if device:
+        cases, controls = torch.from_numpy(cases.view(np.int32)).cuda(), torch.from_numpy(controls.view(np.int32)).cuda()
+    path = str(tmp_path / "run.ckpt")
+    calls = 0
+    while True:
+        r, done, nxt = episdet.search_resumable(cases, controls, nc, nn, path, num_snps=M, order=order, top_k=k,
+                                                engine="tensor", num_slabs=7, max_slabs=2)
+        calls += 1
+        if done:
+            break
+        assert 0 < nxt < M and calls < 8
+    assert calls >= 2
+    assert r.snps == plain.snps and r.score == plain.score and r.score_fp32 == plain.score_fp32
+    assert r.packed_indices == plain.packed_indices and r.sets_evaluated == plain.sets_evaluated
+    assert np.array_equal(r.top_snps, plain.top_snps)
+    assert np.array_equal(r.top_fp32.view(np.uint32), plain.top_fp32.view(np.uint32))
+    assert np.array_equal(r.top_fp64, plain.top_fp64)
+    # A finished checkpoint answers again without searching.
+    again, done, _ = episdet.search_resumable(cases, controls, nc, nn, path, num_snps=M, order=order, top_k=k,
+                                              engine="tensor", num_slabs=7)
+    assert done and again.snps == r.snps and again.kernel_launches == r.kernel_launches
 
 
 def test_batched_equals_plain(episdet):
