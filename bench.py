@@ -62,22 +62,6 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
-def work_slabs(n):
-    """Splits first-SNP indices [0, M-2) into n contiguous slabs of equal C(M-1-x, 2) work."""
-    w = [math.comb(M - 1 - x, 2) for x in range(M - 2)]
-    total = sum(w)
-    bounds, acc, r = [0], 0, 1
-    for x, v in enumerate(w):
-        acc += v
-        if r < n and acc >= total * r / n:
-            bounds.append(x + 1)
-            r += 1
-    while len(bounds) < n:
-        bounds.append(M - 2)
-    bounds.append(M - 2)
-    return [(bounds[i], bounds[i + 1]) for i in range(n)]
-
-
 class Clocks:
     """nvidia-smi sampler (200 ms) covering the timed region."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
@@ -252,22 +236,11 @@ def batched_vs_plain(reps=2):
             "timing": f"wall clock per pass, device-resident planes, best of {reps} after a warm-up pass"}
 
 
-def merge_candidates(tops):
-    """tops: per-rank (top_snps, top_fp32, top_fp64).  Global FP32 top-K by
-    (score, lexicographic set) and the FP64 optimum (lowest set on ties)."""
-    rows = []
-    for snps, f32, f64 in tops:
-        for s, a, b in zip(snps.tolist(), f32.tolist(), f64.tolist()):
-            rows.append((a, tuple(s), b))
-    rows.sort(key=lambda r: (r[0], r[1]))
-    best = min(rows, key=lambda r: (r[2], r[1]))
-    return rows, best
-
-
 def ours(args):
     import numpy as np
     import torch
     import episdet
+    import sharded
 
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
@@ -277,7 +250,7 @@ def ours(args):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     cases, controls = generate()
-    fb, fe = work_slabs(world)[rank]
+    fb, fe = sharded.work_slabs(M, 3, world)[rank]
     stream = torch.cuda.Stream()
     dc = torch.from_numpy(cases.view(np.int32)).cuda()
     dn = torch.from_numpy(controls.view(np.int32)).cuda()
@@ -294,22 +267,8 @@ def ours(args):
     def gather(r):
         if world == 1:
             return [(r.top_snps, r.top_fp32, r.top_fp64)]
-        import torch.distributed as dist
-
-        t = torch.zeros((K, 5), dtype=torch.float64, device="cuda")
-        n = len(r.top_fp32)
-        t[:n, 0:3] = torch.from_numpy(r.top_snps.astype(np.float64))
-        t[:n, 3] = torch.from_numpy(r.top_fp32.astype(np.float64))
-        t[:n, 4] = torch.from_numpy(r.top_fp64)
-        t[n:, 3] = float("inf")
-        out = [torch.empty_like(t) for _ in range(world)]
-        dist.all_gather(out, t)
-        tops = []
-        for o in out:
-            o = o.cpu().numpy()
-            o = o[np.isfinite(o[:, 3])]
-            tops.append((o[:, 0:3].astype(np.int64), o[:, 3], o[:, 4]))
-        return tops
+        return sharded.gather_candidates(r.top_snps, r.top_fp32, r.top_fp64, K, 3,
+                                         device=torch.device("cuda", local))
 
     def barrier():
         torch.cuda.synchronize()
@@ -351,7 +310,7 @@ def ours(args):
     value = total_sets * (NC + NN) / (ms_step * 1e-3) / 1e12
     value_e2e = total_sets * (NC + NN) / (ms_e2e / args.steps * 1e-3) / 1e12
     r0 = res[-1][0]
-    rows, best = merge_candidates(res[-1][1])
+    rows, best = sharded.merge_candidates(res[-1][1], "k2", K)
     if rank != 0:
         if world > 1:
             import torch.distributed as dist

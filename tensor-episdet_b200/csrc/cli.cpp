@@ -4,6 +4,11 @@
 // stdout lines as src/tensor-episdet.cu:32-206 of hiperbio/tensor-episdet;
 // the search itself goes through the reference-compatible
 // EpistasisDetectionSearch() of compat.cpp.
+//
+// Optional, after the descriptor: `--checkpoint FILE [--slabs N]` runs the
+// search in N slabs (default 16) through episdet_search_resumable, saving
+// the progress to FILE after each slab; rerunning the same command after an
+// interruption continues from FILE.  The output lines are the same.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -13,8 +18,14 @@
 
 #include "episdet.h"
 
+#include <cstdlib>
+#include <cstring>
+
 #ifndef EPISDET_COMPAT_ORDER
 #define EPISDET_COMPAT_ORDER 3
+#endif
+#ifndef EPISDET_COMPAT_SCORE
+#define EPISDET_COMPAT_SCORE EPISDET_SCORE_K2
 #endif
 
 cudaError_t EpistasisDetectionSearch(unsigned int* datasetCases, unsigned int* datasetControls, int numSNPs,
@@ -35,8 +46,18 @@ int main(int argc, const char* argv[]) {
         std::cerr << "Compute capability 10.0 (sm_100a) is required." << std::endl;
         return 1;
     }
+    const char* checkpoint = nullptr;
+    int slabs = 0;
+    for (int i = 2; i < argc; ++i) {
+        if (!std::strcmp(argv[i], "--checkpoint") && i + 1 < argc)
+            checkpoint = argv[++i];
+        else if (!std::strcmp(argv[i], "--slabs") && i + 1 < argc)
+            slabs = std::atoi(argv[++i]);
+        else
+            argc = 0;  // unknown option: print the usage
+    }
     if (argc < 2) {
-        std::cerr << "Usage: tensor-episdet dataset.txt" << std::endl;
+        std::cerr << "Usage: tensor-episdet dataset.txt [--checkpoint FILE [--slabs N]]" << std::endl;
         return 1;
     }
     episdet_dataset d;
@@ -61,10 +82,33 @@ int main(int argc, const char* argv[]) {
     double seconds = 0.0;
     float best = 0.0f;
     unsigned long long packed = 0;
-    e = EpistasisDetectionSearch((unsigned int*)d.cases, (unsigned int*)d.controls, d.num_snps, d.num_cases,
-                                 d.num_controls, numSNPsWithPadding, casesPad, controlsPad, &rounds, &seconds, &best,
-                                 &packed);
-    if (e != cudaSuccess) std::cerr << "Epistasis detection search failed." << std::endl;
+    if (checkpoint) {
+        episdet_options o;
+        episdet_default_options(&o);
+        o.order = EPISDET_COMPAT_ORDER;
+        o.score = EPISDET_COMPAT_SCORE;
+        episdet_resume rs;
+        std::memset(&rs, 0, sizeof(rs));
+        rs.path = checkpoint;
+        rs.num_slabs = slabs;
+        episdet_result r;
+        std::memset(&r, 0, sizeof(r));
+        if (episdet_search_resumable(&d, &o, &rs, &r) != EPISDET_OK || !rs.done) {
+            std::cerr << "Epistasis detection search failed: " << episdet_last_error() << std::endl;
+            e = cudaErrorUnknown;
+        } else {
+            e = cudaSuccess;
+            rounds = (int)r.rounds;
+            seconds = r.seconds;
+            best = (float)r.score;
+            packed = (unsigned long long)r.packed_indices;
+        }
+    } else {
+        e = EpistasisDetectionSearch((unsigned int*)d.cases, (unsigned int*)d.controls, d.num_snps, d.num_cases,
+                                     d.num_controls, numSNPsWithPadding, casesPad, controlsPad, &rounds, &seconds,
+                                     &best, &packed);
+        if (e != cudaSuccess) std::cerr << "Epistasis detection search failed." << std::endl;
+    }
 
 #if EPISDET_COMPAT_ORDER == 3
     std::cout << "-------------------------------" << std::endl

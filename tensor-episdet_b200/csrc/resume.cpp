@@ -281,7 +281,7 @@ extern "C" episdet_status episdet_search_resumable(const episdet_dataset* data, 
                   [maximize](const Entry& x, const Entry& y) { return fp32_before(x, y, maximize); });
         if ((int)s.cands.size() > k) s.cands.resize((size_t)k);
         s.h.sets_evaluated += r.sets_evaluated;
-        s.h.rounds += r.rounds;
+        s.h.rounds = r.rounds;  // the whole search's reference round count, the same for every slab
         s.h.count_kernel_launches += r.count_kernel_launches;
         s.h.h2d_bytes += r.h2d_bytes;
         s.h.d2h_bytes += r.d2h_bytes;

@@ -319,3 +319,21 @@ def test_cli_output(episdet, oracle, tmp_path, variant, order, score):
     assert best.endswith(want), (best, want)
     assert "Num. of rounds processed: %d" % (1 if order == 2 else 70) in lines  # BLOCK_SIZE 256 rounds
     assert any(l.startswith("Unique sets of SNPs evaluated (k=%d): " % order) for l in lines)
+
+
+@pytest.mark.parametrize("variant", ["triplets.k2", "pairs.mi"])
+def test_cli_checkpoint(episdet, tmp_path, variant):
+    """--checkpoint runs the search in slabs through the resumable entry
+    point and prints the plain run's best-set and round lines."""
+    cases, controls = episdet.generate(33, 70, 1800, 1300)
+    path = str(tmp_path / "data.txt")
+    episdet.write_dataset(path, cases, controls, 1800, 1300)
+    exe = os.path.join(ROOT, "tensor-episdet_b200", "bin", f"tensor-episdet.{variant}.bin")
+    plain = subprocess.run([exe, path], capture_output=True, text=True, timeout=300)
+    ck = str(tmp_path / "run.ckpt")
+    slabs = subprocess.run([exe, path, "--checkpoint", ck, "--slabs", "5"], capture_output=True, text=True,
+                           timeout=300)
+    assert plain.returncode == 0 and slabs.returncode == 0, slabs.stderr
+    pick = lambda out: [l for l in out.splitlines() if "SCORE\t->\t{" in l or l.startswith("Num. of rounds")]
+    assert pick(slabs.stdout) == pick(plain.stdout) and len(pick(plain.stdout)) == 2
+    assert os.path.getsize(ck) > 0

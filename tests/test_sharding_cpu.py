@@ -1,15 +1,21 @@
-"""The N-GPU bench path on CPU ranks: first-SNP slabs of equal work, one
-all-gather of the per-rank candidate lists, merge -> the one-rank answer.
+"""The multi-GPU path on CPU ranks (sharded.py): first-SNP slabs of equal
+work, one all-gather of the per-rank candidate lists, merge -> the one-rank
+answer.
 
-Runs two gloo ranks on 127.0.0.1 with the CPU oracle standing in for the GPU
-search of each slab."""
+Runs gloo ranks on 127.0.0.1 with the CPU oracle standing in for the GPU
+search of each slab (the `search` argument of search_sharded)."""
+import math
 import os
 import socket
+import sys
+from types import SimpleNamespace
 
 import numpy as np
 import pytest
 import torch.distributed as dist
 import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def _free_port():
@@ -20,59 +26,82 @@ def _free_port():
     return p
 
 
-def _rank(rank, world, port, out):
-    import sys
-
-    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-    sys.path[:0] = [root, os.path.join(root, "oracle")]
-    import bench
+def _oracle_search(cases, controls, nc, nn, *, num_snps, order, score, top_k, device, first_begin, first_end):
     import pyoracle
+
+    o = pyoracle.search(cases, controls, nc, nn, order=order, score=score, top_k=top_k, first_begin=first_begin,
+                        first_end=first_end)
+    return SimpleNamespace(top_snps=np.array(o["top"], dtype=np.int64).reshape(-1, order), top_fp32=o["top_fp32"],
+                           top_fp64=o["top_fp64"], sets_evaluated=o["sets"])
+
+
+def _rank(rank, world, port, order, score, out):
+    sys.path[:0] = [os.path.join(ROOT, "tensor-episdet_b200"), os.path.join(ROOT, "oracle")]
+    import pyoracle
+    import sharded
 
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
-    rng = np.random.default_rng(3)
-    M = 40
+    rng = np.random.default_rng(3 + order)
+    M = 40 if order == 3 else 90
     g_cases = rng.integers(0, 3, size=(M, 300))
     g_controls = rng.integers(0, 3, size=(M, 280))
     cases, controls = pyoracle.pack(g_cases), pyoracle.pack(g_controls)
-    bench.M = M  # slabs over this small dataset
-    fb, fe = bench.work_slabs(world)[rank]
-    r = pyoracle.search(cases, controls, 300, 280, order=3, score="k2", top_k=32, first_begin=fb, first_end=fe)
-    mine = (np.array(r["top"], dtype=np.int64), r["top_fp32"], r["top_fp64"])
-    allv = [None] * world
-    dist.all_gather_object(allv, mine)
-    rows, best = bench.merge_candidates(allv)
+    r = sharded.search_sharded(cases, controls, 300, 280, num_snps=M, order=order, score=score, top_k=32,
+                               search=_oracle_search)
     if rank == 0:
-        full = pyoracle.search(cases, controls, 300, 280, order=3, score="k2", top_k=32)
-        out.put((tuple(best[1]), best[2], tuple(full["best"]), full["best_fp64"],
-                 [r[1] for r in rows[:32]], full["top"], sum(1 for _ in range(1))))
+        full = pyoracle.search(cases, controls, 300, 280, order=order, score=score, top_k=32)
+        out.put((tuple(r.snps), r.score, tuple(full["best"]), full["best_fp64"], [tuple(t) for t in r.top_snps],
+                 [tuple(t) for t in full["top"]], r.top_fp32.tobytes(), np.asarray(full["top_fp32"]).tobytes(),
+                 r.sets_evaluated, full["sets"]))
     dist.barrier()
     dist.destroy_process_group()
 
 
 def test_work_slabs_balance():
-    import bench
+    sys.path.insert(0, os.path.join(ROOT, "tensor-episdet_b200"))
+    import sharded
 
-    s = bench.work_slabs(4)
-    assert s[0][0] == 0 and s[-1][1] == bench.M - 2
+    M = 4096
+    s = sharded.work_slabs(M, 3, 4)
+    assert s[0][0] == 0 and s[-1][1] == M - 2
     assert all(a[1] == b[0] for a, b in zip(s, s[1:]))
-    import math
-
-    w = [sum(math.comb(bench.M - 1 - x, 2) for x in range(a, b)) for a, b in s]
+    w = [sum(math.comb(M - 1 - x, 2) for x in range(a, b)) for a, b in s]
     assert max(w) / min(w) < 1.01
+    # Pairs, a sub-range, and more ranks than first SNPs.
+    s = sharded.work_slabs(100, 2, 3, first_begin=10, first_end=40)
+    assert s[0][0] == 10 and s[-1][1] == 40
+    s = sharded.work_slabs(5, 3, 6)
+    assert s[-1][1] == 3 and sum(b - a for a, b in s) == 3 and all(b >= a for a, b in s)
 
 
-def test_two_rank_merge_equals_one_rank():
+def test_merge_orders_like_the_engines():
+    sys.path.insert(0, os.path.join(ROOT, "tensor-episdet_b200"))
+    import sharded
+
+    a = (np.array([[0, 1], [2, 3]]), np.array([5.0, 7.0], np.float32), np.array([5.1, 6.9]))
+    b = (np.array([[0, 2], [1, 4]]), np.array([5.0, 6.0], np.float32), np.array([5.05, 6.9]))
+    rows, best = sharded.merge_candidates([a, b], "k2")
+    assert [r[1] for r in rows] == [(0, 1), (0, 2), (1, 4), (2, 3)]
+    assert best[1] == (0, 2)  # FP64 minimum
+    rows, best = sharded.merge_candidates([a, b], "mi", top_k=3)
+    assert [r[1] for r in rows] == [(2, 3), (1, 4), (0, 1)]
+    assert best[1] == (1, 4)  # FP64 maximum 6.9, tie with (2, 3): lower set
+
+
+@pytest.mark.parametrize("world,order,score", [(2, 3, "k2"), (3, 2, "mi")])
+def test_sharded_equals_one_rank(world, order, score):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    procs = [ctx.Process(target=_rank, args=(r, world, port, order, score, q)) for r in range(world)]
     for p in procs:
         p.start()
     res = q.get(timeout=120)
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    best, best64, full_best, full64, top, full_top, _ = res
+    best, best64, full_best, full64, top, full_top, f32, full_f32, sets, full_sets = res
     assert best == full_best and best64 == full64
-    assert [tuple(t) for t in top] == [tuple(t) for t in full_top]
+    assert top == full_top and f32 == full_f32
+    assert sets == full_sets
