@@ -83,10 +83,11 @@ struct LutShared {
 };
 
 // FP32 score of one table, scoring.hpp:5-16 (K2 cell term t[ctrl] + t[case] -
-// t[ctrl+case+1]; MI terms), cells in index order.
-template <int NC, class Lut>
+// t[ctrl+case+1]; MI terms), cells in index order.  SC: the score when fixed
+// at compile time (EPISDET_SCORE_K2 / _MI), -1 to read T.score.
+template <int NC, class Lut, int SC = -1>
 __device__ __forceinline__ float score32_lut(const ScoreTables& T, const Lut& lut, const int* cs, const int* cn) {
-    if (T.score == 0) {
+    if (SC == 0 || (SC < 0 && T.score == 0)) {
         float s = 0.0f;
 #pragma unroll
         for (int c = 0; c < NC; ++c)

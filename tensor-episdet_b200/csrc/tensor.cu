@@ -443,7 +443,8 @@ __device__ __forceinline__ void record_error(int* err, int code) { atomicCAS(err
 // room on every SM sub-partition for a warp of the regrouping kernels, which
 // run beside it on the auxiliary stream (at 168 registers they could not, and
 // the regrouping of the next group only ran in the gaps between launches).
-template <bool PAIR, bool STAGE>
+// SC: the score fixed at compile time (0 = K2, 1 = MI) or -1 (read at run time).
+template <bool PAIR, bool STAGE, int SC = -1>
 __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
     tc_kernel(const __grid_constant__ TmapPack tm, const __grid_constant__ TcParams P) {
     static_assert(PAIR || !STAGE, "staging is a pair-kernel mode");
@@ -472,7 +473,7 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     GroupSm* s_grp = reinterpret_cast<GroupSm*>(smem + C::kSmemGroup);
-    const int mode = P.mode;
+    const int mode = PAIR ? (int)kTriplets : P.mode;  // the pair kernel only counts triplets
     const int nseg = mode == kTriplets ? 4 : 2;
     const int nbuf = 4 / nseg;
     if (threadIdx.x < P.ngroup) {
@@ -710,7 +711,7 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
         const int yl = m >> 1, j_own = m & 1;
         const int zoff = j_own ? 2 : 0;
         const BarNamed bar{1, kEpiThreads};
-        const bool maximize = P.T.score == 1;
+        const bool maximize = SC >= 0 ? SC == 1 : P.T.score == 1;
         const int M = P.D.M;
         LocalTopK<kCap, kEpiThreads> tk{tbuf, s_count, s_thr, P.S.k, etid};
         // The candidate buffer takes at most kEpiPerStep offers per chunk; its
@@ -866,7 +867,7 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                         cn[4] = cnt(1, 1, 1);
                         load_marg3(P.D.marg[1], M, bsnp, mb);
                         derive9(cn, ma[1], mb);
-                        float sc = score32_lut<9>(P.T, lut, cs, cn);
+                        float sc = score32_lut<9, LutShared, SC>(P.T, lut, cs, cn);
                         Cand cd;
                         cd.key = score_key(sc, maximize);
                         cd.pad = 0;
@@ -896,7 +897,7 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                         pair9_from4(yz9, yz, ma[c], mz);
                         derive27(tab[c], xy9[c], xz9, yz9);
                     }
-                    float sc = score32_lut<27>(P.T, lut, tab[0], tab[1]);
+                    float sc = score32_lut<27, LutShared, SC>(P.T, lut, tab[0], tab[1]);
                     Cand cd;
                     cd.key = score_key(sc, maximize);
                     cd.pad = 0;
@@ -964,9 +965,13 @@ static episdet_status make_tmap(CUtensorMap* m, void* base, uint64_t rows, uint6
 episdet_status tensor_init_attributes() {
     CUDA_TRY(cudaFuncSetAttribute(tc_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)Cfg<false>::kSmemTotal));
-    CUDA_TRY(cudaFuncSetAttribute(tc_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CUDA_TRY(cudaFuncSetAttribute(tc_kernel<true, false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)Cfg<true>::kSmemTotal));
-    CUDA_TRY(cudaFuncSetAttribute(tc_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CUDA_TRY(cudaFuncSetAttribute(tc_kernel<true, true, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)Cfg<true, true>::kSmemTotal));
+    CUDA_TRY(cudaFuncSetAttribute(tc_kernel<true, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)Cfg<true>::kSmemTotal));
+    CUDA_TRY(cudaFuncSetAttribute(tc_kernel<true, true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)Cfg<true, true>::kSmemTotal));
     return get_encoder();
 }
@@ -1121,7 +1126,10 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     // Large classes make the staged kernel's early release of segment 0 pay
     // (its MMAs then overlap the epilogue); smaller ones run the plain kernel.
     const bool staged = std::min(D.n[0], D.n[1]) >= kStageClass;
-    auto* const kern = staged ? tc_kernel<true, true> : tc_kernel<true, false>;
+    // One instance per score, so each carries only its own scoring code.
+    const bool mi = T.score == EPISDET_SCORE_MI;
+    auto* const kern = staged ? (mi ? tc_kernel<true, true, 1> : tc_kernel<true, true, 0>)
+                              : (mi ? tc_kernel<true, false, 1> : tc_kernel<true, false, 0>);
     const size_t ksmem = staged ? Cfg<true, true>::kSmemTotal : Cfg<true>::kSmemTotal;
     // CTA pairs: as many clusters of two as can be resident at once.
     int pairs = 0;
