@@ -12,8 +12,8 @@
  *                              fixed at build time there by -DTRIPLETS and
  *                              -DMI_SCORE (Makefile:8-22), are options here.
  *   episdet_search_batched  <- no counterpart (one dataset per process there,
- *                              src/tensor-episdet.cu:159-172); many cohorts in
- *                              one persistent launch.
+ *                              src/tensor-episdet.cu:159-172); many cohorts,
+ *                              run concurrently, in one call.
  *   episdet_search_perm     <- no counterpart (one label vector there); many
  *                              phenotype permutations of one cohort.
  *   episdet_read_dataset    <- the descriptor/.bin loader of
@@ -130,9 +130,13 @@ void episdet_default_options(episdet_options* opts);
 /* Replaces EpistasisDetectionSearch (src/search-pairs.cu:9, src/search-triplets.cu:8). */
 episdet_status episdet_search(const episdet_dataset* data, const episdet_options* opts, episdet_result* result);
 
-/* Many independent cohorts (uneven SNP and sample counts) in one persistent
- * launch over a shared tile queue.  opts[i] gives cohort i's order/score;
- * results[i] receives its answer. */
+/* Many independent cohorts (uneven SNP and sample counts) in one call: up to
+ * four run at a time, largest first, each on its own library stream and
+ * buffers, so one cohort's small launches share the GPU with the others'.
+ * opts[i] gives cohort i's order/score (leave options.stream 0: cohorts on one
+ * caller stream cannot overlap); results[i] receives exactly the answer
+ * episdet_search would give.  The first failing cohort's error is returned,
+ * naming the cohort. */
 episdet_status episdet_search_batched(const episdet_dataset* cohorts, const episdet_options* opts, int32_t count,
                                       episdet_result* results);
 
