@@ -112,7 +112,8 @@ typedef struct episdet_result {
     uint64_t kernel_launches; /* kernels this call launched */
     double count_kernel_ms;   /* EPISDET_FLAG_TIMING: summed device time of the counting launches */
     int64_t count_kernel_launches; /* launches of the counting kernel */
-    double executed_macs;     /* EPISDET_FLAG_TIMING: 8-bit MACs the tensor engine issued (0 for SIMT) */
+    double executed_macs;     /* EPISDET_FLAG_TIMING: MACs the tensor engine issued (u8 for pairs and the
+                                 pair table, e2m1 for triplets; 0 for SIMT) */
     int64_t h2d_bytes;        /* host->device bytes this call copied */
     int64_t d2h_bytes;        /* device->host bytes this call copied */
     /* Optional caller-owned outputs of capacity top_capacity (may be NULL). */
