@@ -35,7 +35,10 @@ def perm(a):
                       "sets": sets, "tera_sets_samples_per_s": sets * n / dt / 1e12,
                       "label0_best": [list(res[0].snps), res[0].score],
                       "null_best_scores": {"min": float(best[1:].min()), "median": float(np.median(best[1:])),
-                                           "max": float(best[1:].max())} if len(res) > 1 else None}))
+                                           "max": float(best[1:].max())} if len(res) > 1 else None,
+                      # Max-statistic adjusted p-values of label 0's five best sets.
+                      "label0_top5_pvalues": [float(p) for p in episdet.perm_pvalues(res, a.score)[:5]]
+                      if len(res) > 1 else None}))
 
 
 def main():
