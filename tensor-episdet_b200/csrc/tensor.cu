@@ -123,7 +123,9 @@ struct TcParams {
 // 112 for a CTA pair (PAIR), where the other CTA of the pair holds the rest.
 template <bool PAIR, bool STAGE = false>
 struct Cfg {
-    static constexpr int kStages = PAIR ? 5 : 4;
+    // Four stages: a fifth would push the staged instance past the 196 KB
+    // carve-out, halving the L1 left for the epilogue's global table reads.
+    static constexpr int kStages = 4;
     static constexpr int kBRows = PAIR ? kZSnpsPair : 128;
     static constexpr int kNSeg = PAIR ? kNPair : 128;      // accumulator columns per count segment
     static constexpr int kZSnps = PAIR ? kZSnpsPair : kTileSnps;  // B SNPs per tile
