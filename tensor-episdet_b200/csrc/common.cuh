@@ -189,6 +189,7 @@ __device__ __forceinline__ void pair9_from4(int out[9], const uint4& and4, const
 // first and the threshold is the K-th entry.
 template <int CAP, int NT>
 struct LocalTopK {
+    static_assert(CAP > 0 && (CAP & (CAP - 1)) == 0, "compact() is a bitonic sort over a power-of-two buffer");
     Cand* buf;     // [CAP]
     int* count;    // shared scalar
     Cand* thr;     // shared scalar
