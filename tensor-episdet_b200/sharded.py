@@ -105,13 +105,16 @@ def search_sharded(cases, controls, num_cases: int, num_controls: int, *, num_sn
     """The search of episdet.search sharded over the ranks of `group` (every
     rank calls it with the same arguments and its own GPU `device`).  Returns
     the merged answer on every rank: snps, score, score_fp32, top_snps,
-    top_fp32, top_fp64, sets_evaluated (summed over ranks).  `search`
-    replaces episdet.search (same keyword arguments), e.g. to run the merge
-    logic against another implementation."""
+    top_fp32, top_fp64, sets_evaluated (summed over ranks).  The collective
+    runs on `collective_device` (default: this rank's GPU under NCCL, the CPU
+    under gloo).  `search` replaces episdet.search (same keyword arguments),
+    e.g. to run the merge logic against another implementation."""
     import torch
     import torch.distributed as dist
 
     rank, world = dist.get_rank(group), dist.get_world_size(group)
+    if collective_device is None and dist.get_backend(group) == "nccl":
+        collective_device = torch.device("cuda", device)  # NCCL collectives take device tensors
     M = num_snps if num_snps is not None else int(cases.shape[0])
     fb, fe = work_slabs(M, order, world, kwargs.pop("first_begin", 0), kwargs.pop("first_end", 0))[rank]
     run = search or episdet.search
