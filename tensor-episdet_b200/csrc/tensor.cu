@@ -65,7 +65,8 @@ static_assert(kMaxTopK + kEpiPerStep <= kCap, "candidate buffer too small for on
 constexpr uint64_t kWaitLimitNs = 4000000000ull;
 constexpr uint32_t kIdesc = ptx::idesc_u8(128);
 constexpr uint32_t kIdescPair = ptx::idesc_mxf4(kNPair, 256);  // CTA-pair e2m1 MMA, M = 256, N = 112
-// TMEM of the pair kernel: four 112-column count segments, then the block
+// TMEM of the pair kernel: four 112-column count segments (triplets: one
+// accumulator set of four; pairs: two sets of two), then the block
 // scale factors (every byte 1.0 = UE8M0 127) in columns kSfCol .. 511.
 constexpr uint32_t kSfCol = 4 * kNPair;
 
@@ -185,6 +186,33 @@ __global__ void __launch_bounds__(256) unpack_kernel(DevData D, uint8_t* __restr
             o[e] = ((n >> 3) & 1u) | ((n << 6) & 0x100u) | ((n << 15) & 0x10000u) | ((n << 24) & 0x1000000u);
         }
         *reinterpret_cast<uint4*>(out + (size_t)r * pitch + k) = make_uint4(o[0], o[1], o[2], o[3]);
+    }
+}
+
+// Packed planes -> packed e2m1 operand rows of the 2-way pair kernel, in the
+// class-region layout of the regrouped triplet rows (no regrouping): row
+// r = 2*snp + g holds the cases from packed sample 0 and the controls from
+// packed sample Kc + kClassPad, 1.0 (nibble 2) for a set bit, two samples per
+// byte with the even one in the low nibble.  One thread per source word.
+__global__ void __launch_bounds__(256) pack_f4_kernel(DevData D, uint8_t* __restrict__ out, int rows, int pitch) {
+    const int W0 = D.W[0], W1 = D.W[1], wpr = W0 + W1;
+    const int base1 = (W0 * 32 + kClassPad) / 2;  // byte offset of the controls' region
+    const long total = (long)rows * wpr;
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+        const int r = (int)(t / wpr), w = (int)(t % wpr);
+        const int c = w < W0 ? 0 : 1;
+        const int ww = w - (c ? W0 : 0);
+        const uint32_t word = __ldg(D.bits[c] + (size_t)r * D.W[c] + ww);  // sample ww*32 + i at bit 31 - i
+        uint32_t o[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            uint32_t v = 0;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) v |= ((word >> (31 - (8 * e + i))) & 1u) << (4 * i + 1);
+            o[e] = v;
+        }
+        *reinterpret_cast<uint4*>(out + (size_t)r * pitch + (c ? base1 : 0) + (size_t)ww * 16) =
+            make_uint4(o[0], o[1], o[2], o[3]);
     }
 }
 
@@ -446,10 +474,13 @@ __device__ __forceinline__ void record_error(int* err, int code) { atomicCAS(err
 // run beside it on the auxiliary stream (at 168 registers they could not, and
 // the regrouping of the next group only ran in the gaps between launches).
 // SC: the score fixed at compile time (0 = K2, 1 = MI) or -1 (read at run time).
-template <bool PAIR, bool STAGE, int SC = -1>
+// TWO: the pair kernel scoring pairs (two class segments, two accumulator sets)
+// instead of counting triplets.
+template <bool PAIR, bool STAGE, int SC = -1, bool TWO = false>
 __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
     tc_kernel(const __grid_constant__ TmapPack tm, const __grid_constant__ TcParams P) {
     static_assert(PAIR || !STAGE, "staging is a pair-kernel mode");
+    static_assert(!TWO || (PAIR && !STAGE), "the 2-way pair kernel is the plain pair instance");
     using C = Cfg<PAIR, STAGE>;
     constexpr int kStages = C::kStages;
     constexpr int kStageBytes = C::kStageBytes;
@@ -475,7 +506,7 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     GroupSm* s_grp = reinterpret_cast<GroupSm*>(smem + C::kSmemGroup);
-    const int mode = PAIR ? (int)kTriplets : P.mode;  // the pair kernel only counts triplets
+    const int mode = PAIR ? (TWO ? (int)kPairsScore : (int)kTriplets) : P.mode;
     const int nseg = mode == kTriplets ? 4 : 2;
     const int nbuf = 4 / nseg;
     if (threadIdx.x < P.ngroup) {
@@ -646,10 +677,10 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                 // The other segments wait for the whole accumulator set to be
                 // drained by both CTAs' epilogues.
                 const int late_at = (STAGE && gs.stage_ok) ? 1 : 0;
-                const uint32_t dbase = tmem + (uint32_t)(b * nseg * 128);
+                const uint32_t dbase = tmem + (uint32_t)(b * nseg * C::kNSeg);
                 for (int s = 0; ok && s < nseg; ++s) {
                     if (s == late_at) {
-                        const bool freed = PAIR ? ptx::mbar_wait_cluster(&tempty[0], (use & 1) ^ 1, abort, kWaitLimitNs)
+                        const bool freed = PAIR ? ptx::mbar_wait_cluster(&tempty[b], (use & 1) ^ 1, abort, kWaitLimitNs)
                                                 : ptx::mbar_wait(&tempty[b], (use & 1) ^ 1, abort, kWaitLimitNs);
                         if (!freed) {
                             ok = false;
@@ -748,7 +779,7 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
             const bool stg = STAGE && s_grp[g].stage_ok;
             // This thread's A SNP (pairs: a, triplets: Y); a pair tile spans 128 A SNPs.
             const int arow = PAIR ? tl.x * 2 * kTileSnps + rank * kTileSnps + yl : tl.x * kTileSnps + yl;
-            const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * nseg * 128);
+            const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * nseg * C::kNSeg);
             if constexpr (STAGE) {
                 if (stg) {
                     // Copy this thread's columns of segment 0 to shared memory
@@ -975,6 +1006,10 @@ episdet_status tensor_init_attributes() {
                                   (int)Cfg<true>::kSmemTotal));
     CUDA_TRY(cudaFuncSetAttribute(tc_kernel<true, true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)Cfg<true, true>::kSmemTotal));
+    CUDA_TRY(cudaFuncSetAttribute(tc_kernel<true, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)Cfg<true>::kSmemTotal));
+    CUDA_TRY(cudaFuncSetAttribute(tc_kernel<true, false, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)Cfg<true>::kSmemTotal));
     return get_encoder();
 }
 
@@ -997,16 +1032,6 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     const int Kc = D.W[0] * 32, Kn = D.W[1] * 32;
     const int pitch2 = Kc + Kn;
     const int rows = 2 * M;
-    CUDA_TRY(w->planes8.ensure((size_t)rows * pitch2));
-    uint8_t* P2 = (uint8_t*)w->planes8.p;
-    unpack_kernel<<<grid_for((long)rows * (pitch2 / 16), 256), 256, 0, w->st>>>(D, P2, rows, pitch2);
-    CHECK_LAUNCH();
-    ++*launches;
-    TmapPack tm2;
-    memset(&tm2, 0, sizeof(tm2));
-    st = make_tmap(&tm2.m[0], P2, (uint64_t)rows, (uint64_t)pitch2);
-    if (st != EPISDET_OK) return st;
-
     const int nt = (M + kTileSnps - 1) / kTileSnps;
     const int bs_lines = (M + 255) / 256;
     std::vector<int2> tiles;
@@ -1018,31 +1043,81 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     p.first_begin = fb;
     p.first_end = fe;
     p.err = d_err;
-    p.seg2[0] = Seg{0, Kc / kKB};
-    p.seg2[1] = Seg{Kc / kKB, pitch2 / kKB};
+    const bool mi = T.score == EPISDET_SCORE_MI;
 
     if (o.order == 2) {
-        for (int a = fb / kTileSnps; a <= (fe - 1) / kTileSnps; ++a)
-            for (int b = a; b < nt; ++b) tiles.push_back(make_int2(a, b));
+        // Pairs on the CTA-pair kind::mxf4 kernel: packed e2m1 rows of every
+        // SNP plane, tiles of 128 A SNPs x 56 B SNPs whose B range reaches
+        // past the tile's first A SNP, two accumulator sets in TMEM.
+        const int pitchx = (Kc + kClassPad) / 2 + (Kn + kClassPad) / 2;
+        CUDA_TRY(w->xsub[0].ensure((size_t)rows * pitchx));
+        uint8_t* F = (uint8_t*)w->xsub[0].p;
+        pack_f4_kernel<<<grid_for((long)rows * (D.W[0] + D.W[1]), 256), 256, 0, w->st>>>(D, F, rows, pitchx);
+        CHECK_LAUNCH();
+        ++*launches;
+        TmapPack tmf;
+        memset(&tmf, 0, sizeof(tmf));
+        st = make_tmap(&tmf.m[0], F, (uint64_t)rows, (uint64_t)pitchx);
+        if (st != EPISDET_OK) return st;
+        st = make_tmap(&tmf.m[kMaxGroup], F, (uint64_t)rows, (uint64_t)pitchx, kZSnpsPair);
+        if (st != EPISDET_OK) return st;
+        const int ntb = (M + kZSnpsPair - 1) / kZSnpsPair;
+        for (int a = fb / (2 * kTileSnps); a <= (fe - 1) / (2 * kTileSnps); ++a)
+            for (int bt = (2 * kTileSnps * a) / kZSnpsPair; bt < ntb; ++bt) tiles.push_back(make_int2(a, bt));
         CUDA_TRY(w->tiles.ensure(sizeof(int2) * tiles.size()));
         CUDA_TRY(cudaMemcpyAsync(w->tiles.p, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice, w->st));
         if (progress)
             for (int i = 0; i < bs_lines; ++i) printf("Outer loop iteration %d out of %d\n", i, bs_lines);
         w->h2d += (int64_t)(sizeof(int2) * tiles.size());
+        const int kb1 = (Kc + kClassPad) / kF4PerKB;
+        p.seg2[0] = Seg{0, (D.n[0] + kF4PerKB - 1) / kF4PerKB};
+        p.seg2[1] = Seg{kb1, kb1 + (D.n[1] + kF4PerKB - 1) / kF4PerKB};
         p.ngroup = 1;
         p.grp[0] = GroupDesc{(const int2*)w->tiles.p, 0, -1, nullptr};
         p.ntiles = (int)tiles.size();
         p.mode = kPairsScore;
+        auto* const kern2 = mi ? tc_kernel<true, false, 1, true> : tc_kernel<true, false, 0, true>;
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 2;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(2 * (grid / 2), 1, 1);
+        cfg.blockDim = dim3(kThreads, 1, 1);
+        cfg.dynamicSmemBytes = Cfg<true>::kSmemTotal;
+        cfg.stream = w->st;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int pairs = 0;
+        CUDA_TRY(cudaOccupancyMaxActiveClusters(&pairs, kern2, &cfg));
+        pairs = std::min(pairs, grid / 2);
+        if (pairs < 1) return set_error(EPISDET_ERR_UNSUPPORTED, "no CTA pair of the counting kernel fits on the device");
+        // No more clusters than tiles: SMs left idle stay free for concurrent work.
+        cfg.gridDim = dim3(2 * std::max(1, std::min(pairs, (int)tiles.size())), 1, 1);
         CUDA_TRY(timer_begin(w));
-        // No more CTAs than tiles: SMs left idle stay free for concurrent work.
-        const int g2 = std::max(1, std::min(grid, (int)tiles.size()));
-        tc_kernel<false, false><<<g2, kThreads, Cfg<false>::kSmemTotal, w->st>>>(tm2, p);
+        CUDA_TRY(cudaLaunchKernelEx(&cfg, kern2, tmf, p));
         CHECK_LAUNCH();
         CUDA_TRY(timer_end(w));
         ++*launches;
-        if (w->timing) w->executed_macs = (double)tiles.size() * kTileRows * kTileRows * (double)pitch2;
+        if (w->timing)
+            w->executed_macs = (double)tiles.size() * 2.0 * kTileRows * kNPair *
+                               (double)(p.seg2[0].kb1 - p.seg2[0].kb0 + p.seg2[1].kb1 - p.seg2[1].kb0) * kF4PerKB;
         return EPISDET_OK;
     }
+
+    CUDA_TRY(w->planes8.ensure((size_t)rows * pitch2));
+    uint8_t* P2 = (uint8_t*)w->planes8.p;
+    unpack_kernel<<<grid_for((long)rows * (pitch2 / 16), 256), 256, 0, w->st>>>(D, P2, rows, pitch2);
+    CHECK_LAUNCH();
+    ++*launches;
+    TmapPack tm2;
+    memset(&tm2, 0, sizeof(tm2));
+    st = make_tmap(&tm2.m[0], P2, (uint64_t)rows, (uint64_t)pitch2);
+    if (st != EPISDET_OK) return st;
+
+    p.seg2[0] = Seg{0, Kc / kKB};
+    p.seg2[1] = Seg{Kc / kKB, pitch2 / kKB};
 
     // 3-way: pair table of every SNP pair whose first index is in a tile >= fb's.
     for (int c = 0; c < 2; ++c) {
@@ -1129,7 +1204,6 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     // (its MMAs then overlap the epilogue); smaller ones run the plain kernel.
     const bool staged = std::min(D.n[0], D.n[1]) >= kStageClass;
     // One instance per score, so each carries only its own scoring code.
-    const bool mi = T.score == EPISDET_SCORE_MI;
     auto* const kern = staged ? (mi ? tc_kernel<true, true, 1> : tc_kernel<true, true, 0>)
                               : (mi ? tc_kernel<true, false, 1> : tc_kernel<true, false, 0>);
     const size_t ksmem = staged ? Cfg<true, true>::kSmemTotal : Cfg<true>::kSmemTotal;
