@@ -1,25 +1,31 @@
 // tensor.cu -- tcgen05 (5th-generation tensor core) counting engine.
 //
-// Counting is a matrix product over 0/1 bytes: every {SNP, genotype} bit
-// plane row is unpacked once to bytes, so that for rows a, b the u8 x u8 -> s32
-// product sum_s a[s]*b[s] is the AND-popcount the reference computes as
-// (popc a + popc b - popc(a^b))/2 from its CUTLASS XOR GEMM
-// (src/helper.cu:636-637, :484-485, :714-750).
+// Counting is a matrix product over 0/1 operand rows: for rows a, b (one per
+// {SNP, genotype} bit plane) sum_s a[s]*b[s] is the AND-popcount the reference
+// computes as (popc a + popc b - popc(a^b))/2 from its CUTLASS XOR GEMM
+// (src/helper.cu:636-637, :484-485, :714-750).  Two operand forms:
+//   * packed e2m1 (1.0 = nibble 2, two samples per byte), multiplied by
+//     tcgen05.mma.cta_group::2.kind::mxf4 with unit block scales and FP32
+//     accumulation (exact below 2^24): the pair kernel tc_kernel<true, ...>,
+//     used for triplets and for the 2-way search;
+//   * 0/1 bytes, multiplied by tcgen05.mma.cta_group::1.kind::i8 (u8 x u8 ->
+//     s32): tc_kernel<false, ...>, used for the 3-way pair table.
 //
 // Pipeline per CTA (one CTA per SM, persistent over a tile list):
-//   warp 0      TMA producer: 128x128-byte tiles of the A and B row blocks,
+//   warp 0      TMA producer: 128-byte K blocks of the A and B row blocks,
 //               128-byte swizzle, 4-stage mbarrier ring (no multicast).
-//   warp 1      MMA issuer: tcgen05.mma.cta_group::1.kind::i8, M=N=128,
-//               K=32 per instruction, accumulators in TMEM (512 columns).
-//   warps 2..5  epilogue: tcgen05.ld of the counts, derivation of the 9 / 27
+//   warp 1      MMA issuer (the even CTA of a pair issues for both),
+//               accumulators in TMEM (512 columns).
+//   warps 2..9  epilogue: tcgen05.ld of the counts, derivation of the 9 / 27
 //               contingency cells, K2 / MI score, per-CTA top-K candidates.
 //               No count ever returns to HBM.
 //
-// Tiles are 64 SNPs x 2 planes = 128 rows on both sides; accumulators are
-// kept per K segment:
-//   pairs:    segments {cases, controls}                 -> 2 x 128 columns
+// Pair-kernel tiles are M = 256 A rows (128 SNPs x 2 planes; each CTA holds
+// 128 rows = 64 SNPs) by N = 112 B rows (56 SNPs x 2 planes; each CTA loads 56
+// of them); counts are kept per K segment:
+//   pairs:    segments {cases, controls}                 -> 2 x 112 columns, two sets
 //   triplets: segments {cases, controls} x {X genotype a, X genotype b}
-//                                                        -> 4 x 128 columns
+//                                                        -> 4 x 112 columns, one set
 // For triplets the sample columns are regrouped per first SNP X by X's
 // genotype (xinfo/compact kernels below), keeping the two genotypes of X with
 // the fewest samples; the third is recovered from the Y-Z pair table exactly
