@@ -472,9 +472,11 @@ __global__ void __launch_bounds__(kCmpThreads, 8)
 __device__ __forceinline__ void record_error(int* err, int code) { atomicCAS(err, 0, code); }
 
 // ------------------------------------------------------------------ kernel
-// PAIR: launched as clusters of two CTAs that share each M = 256 x N = 128
-// tile (cta_group::2): the even CTA's MMA warp issues for both, each CTA holds
-// the accumulators of its 128 A rows and scores them.  Triplet mode only.
+// PAIR: launched as clusters of two CTAs that share each M = 256 x N = 112
+// kind::mxf4 tile (cta_group::2): the even CTA's MMA warp issues for both,
+// each CTA holds the accumulators of its 128 A rows and scores them; triplets,
+// or pairs with TWO.  Without PAIR: the kind::i8 single-CTA kernel (pair
+// table).  STAGE: count segment 0 is copied out of TMEM early (triplets).
 // The pair kernel is held to 144 registers a thread: its ten warps then leave
 // room on every SM sub-partition for a warp of the regrouping kernels, which
 // run beside it on the auxiliary stream (at 168 registers they could not, and
