@@ -66,9 +66,9 @@ def test_config1_pairs_k2(episdet, oracle, engine):
 
 @pytest.mark.parametrize("score", ["k2", "mi"])
 def test_large_classes_triplets(episdet, oracle, score):
-    """Classes of >= 65,536 samples: the triplet launches use the kernel that
+    """Classes of >= 32,768 samples: the triplet launches use the kernel that
     copies count segment 0 out of TMEM early; first SNPs whose segment 0 holds
-    fewer than 16,384 samples (low MAF) run it without the copy, so both paths
+    fewer than 8,192 samples (low MAF) run it without the copy, so both paths
     meet in one launch."""
     cases, controls = episdet.generate(0xE91A, 44, 70000, 66000, maf=(0.02, 0.5))
     k = 256
