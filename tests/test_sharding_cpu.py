@@ -105,3 +105,30 @@ def test_sharded_equals_one_rank(world, order, score):
     assert best == full_best and best64 == full64
     assert top == full_top and f32 == full_f32
     assert sets == full_sets
+
+
+@pytest.mark.parametrize("score", ["k2", "mi"])
+def test_slab_topk_lists_merge_to_the_global_topk(score):
+    """The property the sharded search and the resume cursor rely on: keeping
+    each slab's top-k by (FP32 key, set) and merging the kept lists gives the
+    top-k of the whole set of candidates, ties on the FP32 score included."""
+    sys.path.insert(0, os.path.join(ROOT, "tensor-episdet_b200"))
+    import sharded
+
+    rng = np.random.default_rng(11)
+    for trial in range(20):
+        n = int(rng.integers(50, 400))
+        sets = rng.choice(10**6, size=n, replace=False)
+        snps = np.stack([sets // 10000, (sets // 100) % 100, sets % 100], axis=1)
+        f32 = rng.integers(0, 40, size=n).astype(np.float32) * np.float32(0.5)  # many ties
+        f64 = f32.astype(np.float64) + rng.normal(0, 0.01, size=n)
+        k = int(rng.integers(1, 60))
+        rows_all, best_all = sharded.merge_candidates([(snps, f32, f64)], score, k)
+        cuts = np.sort(rng.choice(np.arange(1, n), size=int(rng.integers(1, 6)), replace=False))
+        parts = []
+        for idx in np.split(np.arange(n), cuts):
+            r, _ = sharded.merge_candidates([(snps[idx], f32[idx], f64[idx])], score, k)
+            parts.append((np.array([x[1] for x in r]).reshape(-1, 3), np.array([x[0] for x in r], np.float32),
+                          np.array([x[2] for x in r])))
+        rows, best = sharded.merge_candidates(parts, score, k)
+        assert rows == rows_all and best == best_all
