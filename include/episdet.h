@@ -66,6 +66,14 @@ enum { EPISDET_ENGINE_AUTO = 0, EPISDET_ENGINE_TENSOR = 1, EPISDET_ENGINE_SIMT =
 #define EPISDET_FLAG_PROGRESS 0x1u     /* print the reference's "Outer loop iteration" lines */
 #define EPISDET_FLAG_NO_VALIDATE 0x2u  /* skip the padding / plane-overlap check */
 #define EPISDET_FLAG_TIMING 0x4u       /* time every counting-kernel launch (result.count_kernel_ms) */
+/* Pick the triplet kernel instance for this shape by measurement: the first
+ * search of a shape (order, score, log2 of the smaller class) times the plain
+ * and the segment-staging instance on the first 8 first SNPs of its own data
+ * and keeps the faster; the choice is cached for the process and, when the
+ * environment variable EPISDET_TUNE_CACHE names a file, read from and appended
+ * to it.  Without the flag the instance follows a fixed rule (staging from
+ * classes of 32,768 samples).  Results are the same either way. */
+#define EPISDET_FLAG_AUTOTUNE 0x8u
 
 /* One cohort split into cases and controls (the reference's two .bin files). */
 typedef struct episdet_dataset {
@@ -230,6 +238,10 @@ episdet_status episdet_generate_cohort(uint64_t seed, int32_t num_snps, int32_t 
  * num_cases individuals), the others are seeded random permutations of it. */
 episdet_status episdet_generate_labels(uint64_t seed, int32_t num_samples, int32_t num_cases, int32_t num_labels,
                                        uint32_t* labels);
+
+/* The cached EPISDET_FLAG_AUTOTUNE choice for a shape: 1 = segment-staging
+ * triplet instance, 0 = plain instance, -1 = not tuned yet. */
+int32_t episdet_tuned_stage(int32_t order, int32_t score, int32_t num_cases, int32_t num_controls);
 
 uint64_t episdet_n_choose_k(uint32_t n, uint32_t k);
 const char* episdet_status_string(episdet_status s);

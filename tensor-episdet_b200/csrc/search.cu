@@ -12,7 +12,9 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -444,10 +446,96 @@ extern "C" void episdet_default_options(episdet_options* o) {
 namespace episdet {
 
 // The body of one search; the caller holds w->mu and has validated o.
+// ------------------------------------------------------------ autotuning
+// The measured choice of triplet instance per shape (EPISDET_FLAG_AUTOTUNE),
+// kept for the process and, when EPISDET_TUNE_CACHE names a file, read from it
+// once and appended to it: one "order score bucket choice" line per shape,
+// bucket = floor(log2(smaller class)).
+static std::mutex g_tune_mu;
+static std::map<int, int> g_tune;
+static bool g_tune_loaded = false;
+
+static int tune_key(int order, int score, int nc, int nn) {
+    int m = std::max(1, std::min(nc, nn)), b = 0;
+    while (m >>= 1) ++b;
+    return (order << 16) | (score << 8) | b;
+}
+
+static void tune_load_locked() {
+    if (g_tune_loaded) return;
+    g_tune_loaded = true;
+    const char* path = std::getenv("EPISDET_TUNE_CACHE");
+    FILE* f = path && *path ? std::fopen(path, "r") : nullptr;
+    if (!f) return;
+    char line[128];
+    while (std::fgets(line, sizeof(line), f)) {
+        int order, score, bucket, choice;
+        if (std::sscanf(line, "%d %d %d %d", &order, &score, &bucket, &choice) == 4 && (choice == 0 || choice == 1) &&
+            order >= 2 && order <= 3 && score >= 0 && score <= 1 && bucket >= 0 && bucket < 64)
+            g_tune[(order << 16) | (score << 8) | bucket] = choice;
+    }
+    std::fclose(f);
+}
+
+static int tune_lookup(int key) {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    tune_load_locked();
+    auto it = g_tune.find(key);
+    return it == g_tune.end() ? -1 : it->second;
+}
+
+static void tune_store(int key, int choice) {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    tune_load_locked();
+    g_tune[key] = choice;
+    const char* path = std::getenv("EPISDET_TUNE_CACHE");
+    if (FILE* f = path && *path ? std::fopen(path, "a") : nullptr) {
+        std::fprintf(f, "%d %d %d %d\n", key >> 16, (key >> 8) & 0xFF, key & 0xFF, choice);
+        std::fclose(f);
+    }
+}
+
+// Times both triplet instances on the first 8 first SNPs of this search (two
+// rounds, alternating, minimum per instance) and returns the faster.
+static episdet_status tune_probe(Workspace* w, const episdet_dataset* data, const episdet_options& o, int* choice) {
+    episdet_options po = o;
+    po.flags = (o.flags & ~(EPISDET_FLAG_AUTOTUNE | EPISDET_FLAG_PROGRESS)) | EPISDET_FLAG_TIMING;
+    po.first_begin = 0;
+    po.first_end = std::min(data->num_snps, 8);
+    double best[2] = {1e300, 1e300};
+    for (int round = 0; round < 2; ++round)
+        for (int c = 0; c < 2; ++c) {
+            episdet_result r;
+            memset(&r, 0, sizeof(r));
+            w->stage_override = c;
+            episdet_status st = search_locked(w, data, po, &r);
+            w->stage_override = -1;
+            if (st != EPISDET_OK) return st;
+            best[c] = std::min(best[c], r.count_kernel_ms);
+        }
+    *choice = best[1] < best[0] ? 1 : 0;
+    return EPISDET_OK;
+}
+
 episdet_status search_locked(Workspace* w, const episdet_dataset* data, const episdet_options& o,
                              episdet_result* result) {
     auto t0 = std::chrono::steady_clock::now();
     CUDA_TRY(cudaSetDevice(o.device));
+    // Triplet instance for this call; reset on every return.
+    struct Override {
+        Workspace* w;
+        ~Override() { w->stage_override = -1; }
+    } reset{w};
+    if ((o.flags & EPISDET_FLAG_AUTOTUNE) && o.order == 3 && o.engine != EPISDET_ENGINE_SIMT) {
+        const int key = tune_key(o.order, o.score, data->num_cases, data->num_controls);
+        int choice = tune_lookup(key);
+        if (choice < 0) {
+            episdet_status st = tune_probe(w, data, o, &choice);
+            if (st != EPISDET_OK) return st;
+            tune_store(key, choice);
+        }
+        w->stage_override = choice;
+    }
     begin_call(w, o);
     uint32_t* keep_snps = result->top_snps;
     float* keep32 = result->top_fp32;
@@ -549,4 +637,8 @@ extern "C" episdet_status episdet_release_workspace(int32_t device) {
         w->release_all();
     }
     return EPISDET_OK;
+}
+
+extern "C" int32_t episdet_tuned_stage(int32_t order, int32_t score, int32_t num_cases, int32_t num_controls) {
+    return episdet::tune_lookup(episdet::tune_key(order, score, num_cases, num_controls));
 }

@@ -62,6 +62,7 @@ struct Workspace {
     int64_t count_launches = 0;
     double executed_macs = 0.0;
     int tab_score = -1, tab_nc = -1, tab_nn = -1;
+    int stage_override = -1;  // triplet instance: -1 by the class-size rule, 0 plain, 1 staged
     float inv32 = 0.0f, hy32 = 0.0f;
     double inv64 = 0.0, hy64 = 0.0;
 

@@ -1210,7 +1210,7 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     p.mode = kTriplets;
     // Large classes make the staged kernel's early release of segment 0 pay
     // (its MMAs then overlap the epilogue); smaller ones run the plain kernel.
-    const bool staged = std::min(D.n[0], D.n[1]) >= kStageClass;
+    const bool staged = w->stage_override >= 0 ? w->stage_override == 1 : std::min(D.n[0], D.n[1]) >= kStageClass;
     // One instance per score, so each carries only its own scoring code.
     auto* const kern = staged ? (mi ? tc_kernel<true, true, 1> : tc_kernel<true, true, 0>)
                               : (mi ? tc_kernel<true, false, 1> : tc_kernel<true, false, 0>);

@@ -23,6 +23,7 @@ SCORE_K2, SCORE_MI = 0, 1
 HOST, DEVICE = 0, 1
 ENGINE_AUTO, ENGINE_TENSOR, ENGINE_SIMT = 0, 1, 2
 FLAG_PROGRESS, FLAG_NO_VALIDATE, FLAG_TIMING = 0x1, 0x2, 0x4
+FLAG_AUTOTUNE = 0x8  # measure the triplet instance per shape and cache the choice
 
 STATUS = {
     0: "EPISDET_OK",
@@ -44,6 +45,7 @@ EXPORTED = [
     "episdet_generate", "episdet_generate_cohort", "episdet_generate_labels", "episdet_n_choose_k",
     "episdet_status_string", "episdet_last_error", "episdet_abi_version", "episdet_release_workspace",
     "episdet_search_pairs_noalloc", "episdet_binarize", "episdet_perm_pvalues", "episdet_search_resumable",
+    "episdet_tuned_stage",
 ]
 
 
@@ -359,6 +361,13 @@ def search_resumable(cases, controls, num_cases: int, num_controls: int, checkpo
     r, bufs = _result_buffers(top_k)
     _check(lib().episdet_search_resumable(ctypes.byref(d), ctypes.byref(o), ctypes.byref(rs), ctypes.byref(r)))
     return _to_result(order, r, bufs), bool(rs.done), int(rs.next_first)
+
+
+def tuned_stage(order: int, score, num_cases: int, num_controls: int) -> int:
+    """The cached FLAG_AUTOTUNE choice for a shape: 1 staged triplet instance,
+    0 plain, -1 not tuned yet."""
+    sc = {"k2": SCORE_K2, "mi": SCORE_MI}[score] if isinstance(score, str) else int(score)
+    return int(lib().episdet_tuned_stage(order, sc, num_cases, num_controls))
 
 
 def perm_pvalues(results, score="k2") -> np.ndarray:

@@ -8,6 +8,7 @@ import ctypes
 import json
 import os
 import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -337,3 +338,33 @@ def test_cli_checkpoint(episdet, tmp_path, variant):
     pick = lambda out: [l for l in out.splitlines() if "SCORE\t->\t{" in l or l.startswith("Num. of rounds")]
     assert pick(slabs.stdout) == pick(plain.stdout) and len(pick(plain.stdout)) == 2
     assert os.path.getsize(ck) > 0
+
+
+def test_autotune_picks_and_caches_an_instance(tmp_path):
+    """EPISDET_FLAG_AUTOTUNE: the first search of a shape times both triplet
+    instances, caches the faster one (one line in EPISDET_TUNE_CACHE) and gives
+    the same answer as a search without the flag; the next search of the same
+    shape reuses the cached choice."""
+    cache = tmp_path / "tune.txt"
+    code = f"""
+import sys
+sys.path.insert(0, {os.path.join(ROOT, "tensor-episdet_b200")!r})
+import numpy as np, episdet
+cases, controls = episdet.generate(0xE91C, 40, 40000, 36000)
+plain = episdet.search(cases, controls, 40000, 36000, order=3, top_k=128, engine="tensor")
+assert episdet.tuned_stage(3, "k2", 40000, 36000) == -1
+tuned = episdet.search(cases, controls, 40000, 36000, order=3, top_k=128, engine="tensor", flags=episdet.FLAG_AUTOTUNE)
+choice = episdet.tuned_stage(3, "k2", 40000, 36000)
+assert choice in (0, 1), choice
+again = episdet.search(cases, controls, 40000, 36000, order=3, top_k=128, engine="tensor", flags=episdet.FLAG_AUTOTUNE)
+for r in (tuned, again):
+    assert r.snps == plain.snps and r.score == plain.score
+    assert np.array_equal(r.top_snps, plain.top_snps)
+    assert np.array_equal(r.top_fp32.view(np.uint32), plain.top_fp32.view(np.uint32))
+print(choice)
+"""
+    env = dict(os.environ, EPISDET_TUNE_CACHE=str(cache))
+    p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=600)
+    assert p.returncode == 0, p.stderr
+    choice = int(p.stdout.strip().splitlines()[-1])
+    assert cache.read_text().splitlines() == [f"3 0 15 {choice}"]
