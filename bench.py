@@ -194,9 +194,10 @@ def cohorts64():
 
 def batched_vs_plain(reps=2):
     """The 64 cohorts searched one after another through episdet.search (plain)
-    and in one episdet.search_batched call, device-resident planes, wall clock
-    around each full pass (synchronised), best of `reps` after a warm-up pass;
-    every batched result must equal its plain result."""
+    and in one episdet.search_batched call with per-shape autotuning of the
+    triplet instance (the tuning probes run in the warm-up pass), device-resident
+    planes, wall clock around each full pass (synchronised), best of `reps`
+    after a warm-up pass; every batched result must equal its plain result."""
     import numpy as np
     import torch
     import episdet
@@ -210,8 +211,10 @@ def batched_vs_plain(reps=2):
     def plain():
         return [episdet.search(c, k, nc, nn, num_snps=m, **o) for (c, k, nc, nn, m), o in zip(dev, opts)]
 
+    opts_b = [dict(o, flags=episdet.FLAG_AUTOTUNE) for o in opts]
+
     def batched():
-        return episdet.search_batched(dev, opts)
+        return episdet.search_batched(dev, opts_b)
 
     def timed(fn):
         torch.cuda.synchronize()
@@ -233,6 +236,9 @@ def batched_vs_plain(reps=2):
                         "half 2-way half 3-way K2", "plain_s": min(tp), "batched_s": min(tb),
             "ratio": min(tp) / min(tb), "identical": same,
             "plain_rate": work / min(tp) / 1e12, "batched_rate": work / min(tb) / 1e12, "unit": UNIT,
+            "batched_autotune": True,
+            "tuned_staged": sorted({(nc_ if nc_ < nn_ else nn_).bit_length() - 1: episdet.tuned_stage(3, "k2", nc_, nn_)
+                                    for _, _, nc_, nn_, _, o_ in co if o_ == 3}.items()),
             "timing": f"wall clock per pass, device-resident planes, best of {reps} after a warm-up pass"}
 
 
