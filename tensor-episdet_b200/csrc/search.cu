@@ -496,8 +496,15 @@ static void tune_store(int key, int choice) {
 }
 
 // Times both triplet instances on the first 8 first SNPs of this search (two
-// rounds, alternating, minimum per instance) and returns the faster.
+// rounds, alternating, minimum per instance) and returns the staged one only
+// when it is more than 3 % faster (probes share the GPU with any concurrent
+// work).  With fewer cases than segment 0 needs to be staged (it holds cases
+// only), the plain one is taken without a probe.
 static episdet_status tune_probe(Workspace* w, const episdet_dataset* data, const episdet_options& o, int* choice) {
+    if (data->num_cases < kStageMinSamples) {
+        *choice = 0;
+        return EPISDET_OK;
+    }
     episdet_options po = o;
     po.flags = (o.flags & ~(EPISDET_FLAG_AUTOTUNE | EPISDET_FLAG_PROGRESS)) | EPISDET_FLAG_TIMING;
     po.first_begin = 0;
@@ -513,7 +520,7 @@ static episdet_status tune_probe(Workspace* w, const episdet_dataset* data, cons
             if (st != EPISDET_OK) return st;
             best[c] = std::min(best[c], r.count_kernel_ms);
         }
-    *choice = best[1] < best[0] ? 1 : 0;
+    *choice = best[1] < 0.97 * best[0] ? 1 : 0;
     return EPISDET_OK;
 }
 

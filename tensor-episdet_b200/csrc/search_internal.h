@@ -78,6 +78,9 @@ struct Workspace {
 };
 
 constexpr int kMaxLanes = 4;  // concurrent cohorts of one batched call
+// Samples of count segment 0 from which the staged triplet instance copies it
+// out of TMEM early (below, that instance runs like the plain one).
+constexpr int kStageMinSamples = 8192;
 episdet_status get_workspace(int device, Workspace** out);
 episdet_status get_workspace_lane(int device, int lane, Workspace** out);
 episdet_status build_tables(Workspace* w, int score, int nc, int nn, ScoreTables* T);

@@ -91,7 +91,7 @@ struct XInfo {
 };
 
 constexpr int kMaxGroup = 4;  // first SNPs (X) per triplet launch
-constexpr int kStageMin = 8192;     // samples of segment 0 from which the staged kernel copies it out
+constexpr int kStageMin = kStageMinSamples;  // samples of segment 0 from which the staged kernel copies it out
 constexpr int kStageClass = 32768;  // class size from which triplet launches use the staged kernel
 constexpr int kBand = 12;     // tile-band edge of the triplet tile order
 
