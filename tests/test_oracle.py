@@ -168,3 +168,27 @@ def test_fp32_error_with_large_counts(oracle, score):
     assert rel.max() < 1e-5
     best = min(range(len(r["top"])), key=lambda i: (r["top_fp64"][i] * (1 if score == "k2" else -1), r["top"][i]))
     assert tuple(r["best"]) == tuple(r["top"][best])
+
+
+def test_tables_equal_direct_counts_on_random_data(oracle):
+    """The oracle's 9- and 27-cell tables against numpy histograms of the
+    genotype codes, and the cell-sum invariants: a triplet table summed over
+    Z is the (X, Y) pair table, summed over Y and Z it is X's marginal."""
+    rng = np.random.default_rng(23)
+    M, nc, nn = 12, 301, 277
+    g_cases = rng.integers(0, 3, size=(M, nc))
+    g_controls = rng.integers(0, 3, size=(M, nn))
+    cases, controls = oracle.pack(g_cases), oracle.pack(g_controls)
+    m_cases = oracle.marginals(cases, nc)
+    for _ in range(10):
+        x, y, z = sorted(rng.choice(M, size=3, replace=False).tolist())
+        cs3, cn3 = oracle.table3(cases, controls, nc, nn, x, y, z)
+        for got, g in ((cs3, g_cases), (cn3, g_controls)):
+            want = np.bincount(9 * g[x] + 3 * g[y] + g[z], minlength=27)
+            assert got.tolist() == want.tolist()
+        cs2, cn2 = oracle.table2(cases, controls, nc, nn, x, y)
+        assert cs2.tolist() == np.bincount(3 * g_cases[x] + g_cases[y], minlength=9).tolist()
+        assert cn2.tolist() == np.bincount(3 * g_controls[x] + g_controls[y], minlength=9).tolist()
+        assert cs3.reshape(9, 3).sum(axis=1).tolist() == cs2.tolist()
+        assert cn3.reshape(9, 3).sum(axis=1).tolist() == cn2.tolist()
+        assert cs3.reshape(3, 9).sum(axis=1).tolist() == m_cases[:, x].tolist()
