@@ -373,7 +373,8 @@ struct CmpOut {
 
 __global__ void __launch_bounds__(kCmpThreads, 8)
     compact_kernel(DevData D, XWork xw, CmpOut co, int rows_total, int pitch) {
-    __shared__ __align__(16) uint32_t s_src[kCmpDepth][kCmpSpanWords];
+    // One zero word after each span buffer: padding samples read it.
+    __shared__ __align__(16) uint32_t s_src[kCmpDepth][kCmpSpanWords + 4];
     __shared__ int s_lo, s_hi;
     const int mem = (int)blockIdx.z;
     const XInfo* __restrict__ info = xw.info(mem);
@@ -413,6 +414,7 @@ __global__ void __launch_bounds__(kCmpThreads, 8)
     if (threadIdx.x == 0) {
         s_lo = 0x7FFFFFFF;
         s_hi = -1;
+        for (int d = 0; d < kCmpDepth; ++d) s_src[d][kCmpSpanWords] = 0u;
     }
     __syncthreads();
     if (hi >= 0) {
@@ -439,6 +441,14 @@ __global__ void __launch_bounds__(kCmpThreads, 8)
             }
             cp_async_commit();  // one group per row, empty past the end
         };
+        // Per sample, the same for every row: the word of the staged span
+        // (low 16 bits) and the bit's shift (high 16 bits).
+        uint32_t pk[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+            const int s = src[e];
+            pk[e] = s >= 0 ? (uint32_t)((s >> 5) - wlo) | ((uint32_t)(31 - (s & 31)) << 16) : (uint32_t)kCmpSpanWords;
+        }
 #pragma unroll
         for (int d = 0; d < kCmpDepth - 1; ++d) issue(rbeg + d);
         for (int row = rbeg; row < rend; ++row) {
@@ -448,10 +458,8 @@ __global__ void __launch_bounds__(kCmpThreads, 8)
             const uint32_t* sw = s_src[(row - rbeg) % kCmpDepth];
             uint32_t o[2] = {0, 0};
 #pragma unroll
-            for (int e = 0; e < 16; ++e) {
-                const int s = src[e];
-                if (s >= 0) o[e >> 3] |= ((sw[(s >> 5) - wlo] >> (31 - (s & 31))) & 1u) << (4 * (e & 7) + 1);
-            }
+            for (int e = 0; e < 16; ++e)
+                o[e >> 3] |= ((sw[pk[e] & 0xFFFFu] >> (pk[e] >> 16)) & 1u) << (4 * (e & 7) + 1);
             if (kk0 < region) *reinterpret_cast<uint2*>(out + (size_t)row * pitch + colbase) = make_uint2(o[0], o[1]);
         }
         cp_async_wait<0>();
