@@ -143,11 +143,21 @@ def generate():
     return episdet.generate(SEED, M, NC, NN, maf=(0.05, 0.5), planted=[PLANTED], base_risk=0.5, effect=0.25)
 
 
+def generate_oracle():
+    """The same planes made by the oracle library alone (bit-identical to
+    generate(); tests/test_bench_cpu.py checks it), so the reference arm's
+    process never loads the product library."""
+    sys.path.insert(0, ORACLE)
+    import pyoracle
+
+    return pyoracle.generate(SEED, M, NC, NN, maf=(0.05, 0.5), planted=[PLANTED], base_risk=0.5, effect=0.25)
+
+
 def reference_arm(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    cases, controls = generate()
+    cases, controls = generate_oracle()
     ky, cores, run = cpu_sample(cases, controls, target_s=8.0)
     for _ in range(args.warmup):
         run(ky)
@@ -167,7 +177,11 @@ def reference_arm(args):
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference needs CUTLASS 1.3 (absent) and has no CPU path; its algorithm is timed as the "
-                "project's CPU restatement (oracle/)"}))
+                "project's CPU restatement (oracle/), on a bounded sample of the workload (the whole search "
+                "would take hours on the host cores); planes made by the oracle's own generator, so this "
+                "process loads no library of the product",
+        "libraries_loaded": sorted({os.path.relpath(l.split()[-1], ROOT) for l in open("/proc/self/maps")
+                                    if l.rstrip().endswith(".so") and l.split()[-1].startswith(ROOT)})}))
 
 
 # ------------------------------------------------------------------ GPU side

@@ -255,15 +255,19 @@ episdet_status episdet_release_workspace(int32_t device);
  * For callers that cannot let a library allocate device memory: a process
  * whose memory pool or caching allocator already holds the GPU's memory, or a
  * pipeline that cannot take the device-wide synchronisation of cudaFree.
- * Same results as episdet_search with order 2 (same kernels), but every
- * intermediate buffer lives in one fixed 8 MiB device array that the library
- * holds on each GPU that loads it until the process exits.  Limits (beyond
- * them the call returns EPISDET_ERR_INVALID_ARGUMENT): data->memory must be
- * EPISDET_DEVICE, at most 4096 SNPs, 131072 samples (cases + controls) and
- * top_k 1024.  The first call on a device looks up the array's address and
- * should come before any stream capture.  Calls share the array: they are
+ * Same results as episdet_search with order 2 (the same best pair, candidate
+ * list and FP32 / FP64 scores), computed by the integer-pipe (LOP3 + POPC)
+ * pairs kernel rather than the tensor-core one, with every intermediate
+ * buffer in one fixed 8 MiB device array that the library holds on each GPU
+ * that loads it until the process exits.  Limits (beyond them the call
+ * returns EPISDET_ERR_INVALID_ARGUMENT): data->memory must be EPISDET_DEVICE,
+ * at most 4096 SNPs, 131072 samples (cases + controls) and top_k 1024.  The
+ * first call on a device looks up the array's address and should come before
+ * any stream capture; after a cudaDeviceReset of that device the entry point
+ * must not be called again in the process.  Calls share the array: they are
  * serialised by a host lock and each waits for its GPU work before returning,
- * since GPU work of two calls that overlapped would race on it. */
+ * failed calls included, since GPU work of two calls that overlapped would
+ * race on it. */
 episdet_status episdet_search_pairs_noalloc(const episdet_dataset* data, const episdet_options* opts,
                                             episdet_result* result);
 

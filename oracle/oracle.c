@@ -640,3 +640,138 @@ int32_t od_split_by_label(const uint32_t* planes, int32_t M, int32_t n, const ui
     if (num_controls) *num_controls = nn;
     return nc;
 }
+
+/* ------------------------------------------------------------------------
+ * Synthetic datasets, generated here so that a process timing the oracle
+ * (the CPU baseline, the reference arm of bench.py) never loads the product
+ * library.  Bit-identical to episdet_generate by construction: the same
+ * counter-based draws (the SplitMix64 finaliser of Steele, Lea & Flood 2014
+ * applied to (seed, stream, index)), the same Hardy-Weinberg thresholds and
+ * the same penetrance model, so tests can check the two against each other.
+ * ---------------------------------------------------------------------- */
+static uint64_t od_mix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+static uint64_t od_draw(uint64_t seed, uint64_t stream, uint64_t idx) {
+    return od_mix64(od_mix64(seed ^ od_mix64(stream)) ^ idx);
+}
+static double od_u01(uint64_t h) { return (double)(h >> 11) * (1.0 / 9007199254740992.0); }
+
+#define OD_TAG_MAF 0x4D4146ull
+#define OD_TAG_GENO (0x47454E4Full << 24)
+#define OD_TAG_LABEL 0x4C4142ull
+
+static int od_genotype(uint64_t seed, int32_t snp, uint64_t ind, double p) {
+    double u = od_u01(od_draw(seed, OD_TAG_GENO + (uint64_t)snp, ind));
+    double q0 = (1.0 - p) * (1.0 - p);
+    if (u < q0) return 0;
+    if (u < 1.0 - p * p) return 1;
+    return 2;
+}
+
+typedef struct od_fill_arg {
+    uint64_t seed;
+    int32_t M, n, t, nt;
+    const double* maf;
+    const uint64_t* ids;
+    uint32_t* planes;
+} od_fill_arg;
+
+static void* od_fill_worker(void* p) {
+    od_fill_arg* a = (od_fill_arg*)p;
+    size_t W = (size_t)od_class_words(a->n);
+    for (int32_t snp = a->t; snp < a->M; snp += a->nt) {
+        uint32_t* r0 = a->planes + ((size_t)snp * 2) * W;
+        uint32_t* r1 = r0 + W;
+        memset(r0, 0, sizeof(uint32_t) * 2 * W);
+        for (int32_t s = 0; s < a->n; ++s) {
+            int g = od_genotype(a->seed, snp, a->ids[s], a->maf[snp]);
+            if (g < 2) (g == 0 ? r0 : r1)[s / 32] |= 1u << (31 - s % 32);
+        }
+    }
+    return NULL;
+}
+
+static int od_fill(uint64_t seed, int32_t M, const double* maf, const uint64_t* ids, int32_t n, uint32_t* planes,
+                   int threads) {
+    int nt = threads > 0 ? threads : (int)sysconf(_SC_NPROCESSORS_ONLN);
+    if (nt < 1) nt = 1;
+    if (nt > 256) nt = 256;
+    pthread_t th[256];
+    od_fill_arg args[256];
+    for (int i = 0; i < nt; ++i) {
+        args[i] = (od_fill_arg){seed, M, n, i, nt, maf, ids, planes};
+        if (pthread_create(&th[i], NULL, od_fill_worker, &args[i]) != 0) {
+            for (int j = 0; j < i; ++j) pthread_join(th[j], NULL);
+            return -1;
+        }
+    }
+    for (int i = 0; i < nt; ++i) pthread_join(th[i], NULL);
+    return 0;
+}
+
+int od_generate(const od_synth* sp, uint32_t* cases, uint32_t* controls, int threads) {
+    if (!sp || !cases || !controls || sp->num_snps < 1 || sp->num_cases < 1 || sp->num_controls < 1 ||
+        sp->num_planted < 0 || sp->num_planted > 2 || !(sp->maf_min >= 0.0f) || !(sp->maf_max <= 0.5f) ||
+        sp->maf_min > sp->maf_max)
+        return -1;
+    const int32_t M = sp->num_snps;
+    const int ord = sp->planted_order == 2 ? 2 : 3;
+    double* maf = (double*)malloc(sizeof(double) * (size_t)M);
+    uint64_t* cid = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)sp->num_cases);
+    uint64_t* nid = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)sp->num_controls);
+    int rc = 0;
+    if (!maf || !cid || !nid) {
+        rc = -2;
+        goto out;
+    }
+    for (int32_t s = 0; s < M; ++s)
+        maf[s] = (double)sp->maf_min + ((double)sp->maf_max - (double)sp->maf_min) * od_u01(od_draw(sp->seed, OD_TAG_MAF, (uint64_t)s));
+    for (int q = 0; q < sp->num_planted; ++q)
+        for (int e = 0; e < ord; ++e) {
+            int32_t s = sp->planted[q][e];
+            if (s < 0 || s >= M) {
+                rc = -1;
+                goto out;
+            }
+            if (sp->planted_maf > 0.0f) maf[s] = (double)sp->planted_maf;
+        }
+    int32_t nc = 0, nn = 0;
+    if (sp->num_planted == 0) {
+        for (int32_t i = 0; i < sp->num_cases; ++i) cid[nc++] = (uint64_t)i;
+        for (int32_t i = 0; i < sp->num_controls; ++i) nid[nn++] = (uint64_t)(sp->num_cases + i);
+    } else {
+        uint64_t ind = 0;
+        const uint64_t limit = 64ull * (uint64_t)(sp->num_cases + sp->num_controls) + 1000000ull;
+        while (nc < sp->num_cases || nn < sp->num_controls) {
+            if (ind > limit) {
+                rc = -1;
+                goto out;
+            }
+            double risk = (double)sp->base_risk;
+            for (int q = 0; q < sp->num_planted; ++q) {
+                int carried = 1;
+                for (int e = 0; e < ord; ++e) {
+                    int32_t s = sp->planted[q][e];
+                    carried = carried && od_genotype(sp->seed, s, ind, maf[s]) >= 1;
+                }
+                if (carried) risk += (double)sp->effect;
+            }
+            int is_case = od_u01(od_draw(sp->seed, OD_TAG_LABEL, ind)) < risk;
+            if (is_case && nc < sp->num_cases) cid[nc++] = ind;
+            if (!is_case && nn < sp->num_controls) nid[nn++] = ind;
+            ++ind;
+        }
+    }
+    if (od_fill(sp->seed, M, maf, cid, sp->num_cases, cases, threads) != 0 ||
+        od_fill(sp->seed, M, maf, nid, sp->num_controls, controls, threads) != 0)
+        rc = -3;
+out:
+    free(maf);
+    free(cid);
+    free(nid);
+    return rc;
+}

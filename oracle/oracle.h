@@ -115,6 +115,22 @@ int32_t od_split_by_label(const uint32_t* planes, int32_t M, int32_t n, const ui
                           uint32_t* cases_out, uint32_t* controls_out, int32_t* num_controls);
 int32_t od_class_words(int32_t n);
 
+/* Seeded synthetic dataset in the reference format (the generator of the
+ * product library, restated here so that oracle-only processes need no other
+ * library): Hardy-Weinberg genotypes with MAF ~ U[maf_min, maf_max] per SNP,
+ * optional planted sets with penetrance base_risk + effect per set carried
+ * (all SNPs of the set with >= 1 minor allele), individuals drawn in order and
+ * kept while their class has room.  threads <= 0: all online cores. */
+typedef struct od_synth {
+    uint64_t seed;
+    int32_t num_snps, num_cases, num_controls;
+    float maf_min, maf_max;
+    int32_t num_planted, planted_order;
+    int32_t planted[2][3];
+    float planted_maf, base_risk, effect;
+} od_synth;
+int od_generate(const od_synth* spec, uint32_t* cases, uint32_t* controls, int threads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -35,6 +35,14 @@ class _Result(ctypes.Structure):
                 ("sets", ctypes.c_uint64)]
 
 
+class _Synth(ctypes.Structure):
+    _fields_ = [("seed", ctypes.c_uint64), ("num_snps", ctypes.c_int32), ("num_cases", ctypes.c_int32),
+                ("num_controls", ctypes.c_int32), ("maf_min", ctypes.c_float), ("maf_max", ctypes.c_float),
+                ("num_planted", ctypes.c_int32), ("planted_order", ctypes.c_int32),
+                ("planted", (ctypes.c_int32 * 3) * 2), ("planted_maf", ctypes.c_float),
+                ("base_risk", ctypes.c_float), ("effect", ctypes.c_float)]
+
+
 _lib = None
 
 
@@ -63,6 +71,8 @@ def lib() -> ctypes.CDLL:
         L.od_split_by_label.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
                                         ctypes.c_void_p, ctypes.c_void_p, P(ctypes.c_int32)]
         L.od_split_by_label.restype = ctypes.c_int32
+        L.od_generate.argtypes = [P(_Synth), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        L.od_generate.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -107,6 +117,27 @@ def search(cases, controls, nc, nn, order=3, score="k2", top_k=1024, threads=0, 
         "top_fp32": f32[:n].copy(),
         "top_fp64": f64[:n].copy(),
     }
+
+
+def generate(seed, num_snps, num_cases, num_controls, maf=(0.05, 0.5), planted=(), planted_maf=0.0,
+             base_risk=0.5, effect=0.25, threads=0):
+    """The product generator's dataset, made by the oracle library alone
+    (same arguments and bits as episdet.generate)."""
+    s = _Synth()
+    s.seed, s.num_snps, s.num_cases, s.num_controls = seed, num_snps, num_cases, num_controls
+    s.maf_min, s.maf_max = maf
+    s.num_planted = len(planted)
+    s.planted_order = len(planted[0]) if planted else 3
+    for q, ps in enumerate(planted):
+        for e, v in enumerate(ps):
+            s.planted[q][e] = v
+    s.planted_maf, s.base_risk, s.effect = planted_maf, base_risk, effect
+    cases = np.zeros((num_snps, 2, class_words(num_cases)), dtype=np.uint32)
+    controls = np.zeros((num_snps, 2, class_words(num_controls)), dtype=np.uint32)
+    rc = lib().od_generate(ctypes.byref(s), cases.ctypes.data, controls.ctypes.data, threads)
+    if rc != 0:
+        raise ValueError(f"bad synthetic spec ({rc})")
+    return cases, controls
 
 
 def table2(cases, controls, nc, nn, a, b):

@@ -72,6 +72,7 @@ extern "C" episdet_status episdet_search_batched(const episdet_dataset* cohorts,
     for (int32_t i = 0; i < count; ++i) {
         episdet_status st = check_options(&opts[i], cohorts[i].num_snps, &os[i]);
         if (st == EPISDET_OK) st = check_dataset(&cohorts[i], os[i].order);
+        if (st == EPISDET_OK) st = check_engine(&cohorts[i], os[i]);
         if (st != EPISDET_OK) return with_prefix(st, "cohort", i);
         if (os[i].device != os[0].device)
             return set_error(EPISDET_ERR_INVALID_ARGUMENT, "all cohorts of a batch run on one device");

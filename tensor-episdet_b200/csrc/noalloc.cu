@@ -18,7 +18,9 @@
 // All calls share the array and it keeps whatever the last call left in it;
 // the parts that must start at zero are cleared by every call.  Two calls
 // whose GPU work overlapped would race on the array, so calls are serialised
-// by a host lock and each call waits for its GPU work before returning.
+// by a host lock and each call waits for its GPU work before returning, on
+// its error paths too.  The looked-up address is kept for the process: after
+// a cudaDeviceReset of a device the entry point must not be used on it again.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -92,6 +94,9 @@ static episdet_status setup(int device) {
 using namespace episdet;
 using namespace episdet::noalloc;
 
+static episdet_status search_locked(const episdet_dataset* data, const episdet_options& o, uint8_t* S,
+                                    cudaStream_t stream, episdet_result* result);
+
 extern "C" episdet_status episdet_search_pairs_noalloc(const episdet_dataset* data, const episdet_options* opts,
                                                        episdet_result* result) {
     clear_error();
@@ -124,8 +129,18 @@ extern "C" episdet_status episdet_search_pairs_noalloc(const episdet_dataset* da
     CUDA_TRY(cudaSetDevice(o.device));
     st = setup(o.device);
     if (st != EPISDET_OK) return st;
-    uint8_t* S = g_dev_scratch[o.device];
     cudaStream_t stream = (cudaStream_t)(uintptr_t)o.stream;
+    st = search_locked(data, o, g_dev_scratch[o.device], stream, result);
+    // Whatever failed, no GPU work of this call may still use the shared array
+    // once the lock is released (the status of this wait is not the error).
+    if (st != EPISDET_OK) cudaStreamSynchronize(stream);
+    return st;
+}
+
+// The search proper, under g_mu with the device current and the array set up.
+static episdet_status search_locked(const episdet_dataset* data, const episdet_options& o, uint8_t* S,
+                                    cudaStream_t stream, episdet_result* result) {
+    const int M = data->num_snps, nc = data->num_cases, nn = data->num_controls;
 
     uint32_t* keep_snps = result->top_snps;
     float* keep32 = result->top_fp32;

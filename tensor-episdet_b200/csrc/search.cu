@@ -429,6 +429,24 @@ episdet_status check_dataset(const episdet_dataset* d, int order) {
     return EPISDET_OK;
 }
 
+// The tensor engine sums each count over one K segment (a class, or the
+// samples of one class with one genotype of the first SNP) in an FP32
+// accumulator, exact while the segment holds at most 2^24 samples.  Larger
+// classes go to the integer-pipe engine under EPISDET_ENGINE_AUTO and are
+// refused for EPISDET_ENGINE_TENSOR.
+bool tensor_exact_for(const episdet_dataset* d) {
+    return d->num_cases <= kTensorMaxClass && d->num_controls <= kTensorMaxClass;
+}
+
+episdet_status check_engine(const episdet_dataset* d, const episdet_options& o) {
+    if (o.engine == EPISDET_ENGINE_TENSOR && !tensor_exact_for(d))
+        return set_error(EPISDET_ERR_UNSUPPORTED,
+                         "the tensor engine counts a class in FP32 accumulators, exact up to %d samples per class "
+                         "(got %d cases, %d controls); use EPISDET_ENGINE_AUTO or EPISDET_ENGINE_SIMT",
+                         kTensorMaxClass, d->num_cases, d->num_controls);
+    return EPISDET_OK;
+}
+
 }  // namespace episdet
 
 using namespace episdet;
@@ -533,7 +551,10 @@ episdet_status search_locked(Workspace* w, const episdet_dataset* data, const ep
         Workspace* w;
         ~Override() { w->stage_override = -1; }
     } reset{w};
-    if ((o.flags & EPISDET_FLAG_AUTOTUNE) && o.order == 3 && o.engine != EPISDET_ENGINE_SIMT) {
+    episdet_status st0 = check_engine(data, o);
+    if (st0 != EPISDET_OK) return st0;
+    const bool simt = o.engine == EPISDET_ENGINE_SIMT || !tensor_exact_for(data);
+    if ((o.flags & EPISDET_FLAG_AUTOTUNE) && o.order == 3 && !simt) {
         const int key = tune_key(o.order, o.score, data->num_cases, data->num_controls);
         int choice = tune_lookup(key);
         if (choice < 0) {
@@ -565,7 +586,7 @@ episdet_status search_locked(Workspace* w, const episdet_dataset* data, const ep
     CUDA_TRY(cudaEventRecord(w->e0, w->st));
     Slots S;
     bool progress = (o.flags & EPISDET_FLAG_PROGRESS) != 0;
-    if (o.engine == EPISDET_ENGINE_SIMT)
+    if (simt)
         st = run_simt(w, D, T, o, fb, fe, &S, &launches, progress);
     else
         st = run_tensor(w, D, T, o, fb, fe, &S, &launches, progress);
@@ -606,6 +627,8 @@ extern "C" episdet_status episdet_search(const episdet_dataset* data, const epis
     episdet_status st = check_options(opts, data->num_snps, &o);
     if (st != EPISDET_OK) return st;
     st = check_dataset(data, o.order);
+    if (st != EPISDET_OK) return st;
+    st = check_engine(data, o);
     if (st != EPISDET_OK) return st;
     Workspace* w = nullptr;
     st = get_workspace(o.device, &w);

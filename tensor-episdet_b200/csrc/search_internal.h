@@ -88,6 +88,10 @@ episdet_status stage_dataset(Workspace* w, const episdet_dataset* d, bool valida
 episdet_status prepare_slots(Workspace* w, int nslots, int k, Slots* S);
 episdet_status check_options(const episdet_options* in, int M, episdet_options* o);
 episdet_status check_dataset(const episdet_dataset* d, int order);
+// Largest class the tensor engine counts exactly (FP32 accumulators: 2^24).
+constexpr int kTensorMaxClass = 1 << 24;
+bool tensor_exact_for(const episdet_dataset* d);
+episdet_status check_engine(const episdet_dataset* d, const episdet_options& o);
 
 // Brackets one counting-kernel launch with events when timing is on.
 cudaError_t timer_begin(Workspace* w);

@@ -141,3 +141,20 @@ def test_cli_reports_missing_device_and_usage(tmp_path):
     exe = os.path.join(ROOT, "tensor-episdet_b200", "bin", "tensor-episdet.pairs.k2.bin")
     p = subprocess.run([exe], capture_output=True, text=True, timeout=60)
     assert p.returncode == 1
+
+
+def test_tensor_engine_refuses_classes_past_fp32_exactness(episdet):
+    """The tensor engine accumulates a class's counts in FP32, exact up to 2^24
+    samples; a larger class is refused for the tensor engine before any device
+    work (EPISDET_ENGINE_AUTO hands it to the integer-pipe engine instead)."""
+    L = episdet.lib()
+    cases, controls = episdet.generate(1, 10, 64, 64)
+    r = episdet.Result()
+    for big in ((1 << 24) + 1, 1 << 25):
+        for order in (2, 3):
+            o = episdet.make_options(order=order, engine="tensor")
+            d = episdet.Dataset(cases.ctypes.data, controls.ctypes.data, 10, big, 64, 0)
+            assert L.episdet_search(ctypes.byref(d), ctypes.byref(o), ctypes.byref(r)) == 8  # UNSUPPORTED
+            assert b"2^24" in L.episdet_last_error() or b"16777216" in L.episdet_last_error()
+            d = episdet.Dataset(cases.ctypes.data, controls.ctypes.data, 10, 64, big, 0)
+            assert L.episdet_search(ctypes.byref(d), ctypes.byref(o), ctypes.byref(r)) == 8

@@ -22,3 +22,20 @@ def test_reference_arm_json_line():
     cb = d["cpu_baseline"]
     assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
     assert "workload" in d["config"]
+    # The arm runs the oracle alone: no library of the product is mapped.
+    assert d["libraries_loaded"] == ["oracle/build/liboracle.so"], d["libraries_loaded"]
+
+
+def test_oracle_generator_matches_the_product_generator():
+    """The reference arm makes the bench planes with the oracle's generator;
+    they must be the product generator's bits (bench.py's spec, in full)."""
+    sys.path.insert(0, ROOT)
+    import hashlib
+    import numpy as np
+    import bench
+
+    a = bench.generate_oracle()
+    b = bench.generate()
+    for x, y in zip(a, b):
+        assert x.shape == y.shape and x.dtype == y.dtype == np.uint32
+        assert hashlib.sha256(x.tobytes()).hexdigest() == hashlib.sha256(y.tobytes()).hexdigest()
