@@ -74,6 +74,12 @@ enum { EPISDET_ENGINE_AUTO = 0, EPISDET_ENGINE_TENSOR = 1, EPISDET_ENGINE_SIMT =
  * to it.  Without the flag the instance follows a fixed rule (staging from
  * classes of 32,768 samples).  Results are the same either way. */
 #define EPISDET_FLAG_AUTOTUNE 0x8u
+/* Testing aid for failure detection: the tensor engine's scoring warps first
+ * wait for a device word that nothing ever sets, so every counting launch
+ * gives up after wait_limit_ms, drains its copies and MMAs, frees its tensor
+ * memory and returns; the call then fails with EPISDET_ERR_TIMEOUT and the
+ * device stays usable for the next call. */
+#define EPISDET_FLAG_INJECT_STALL 0x10u
 
 /* One cohort split into cases and controls (the reference's two .bin files). */
 typedef struct episdet_dataset {
@@ -103,7 +109,11 @@ typedef struct episdet_options {
     int32_t first_end;    /* 0 -> num_snps */
     uint32_t flags;       /* EPISDET_FLAG_* */
     uint64_t stream;      /* cudaStream_t to run on; 0 = the library's own stream */
-    int32_t reserved[6];
+    /* Longest time one in-kernel wait of the tensor engine (for an operand
+     * copy, an MMA commit, the scoring warps) may take before the launch gives
+     * up and the call returns EPISDET_ERR_TIMEOUT; 0 = 4000 ms. */
+    int32_t wait_limit_ms;
+    int32_t reserved[5];
 } episdet_options;
 
 typedef struct episdet_result {
@@ -250,6 +260,13 @@ int32_t episdet_abi_version(void);
 
 /* Frees the per-device workspace the library keeps between calls. */
 episdet_status episdet_release_workspace(int32_t device);
+
+/* Testing aid for failure detection -- no counterpart in the reference: the
+ * after-th device allocation the library makes from now on (in any thread)
+ * fails as if the device were out of memory, once; the call that needed it
+ * returns EPISDET_ERR_OUT_OF_MEMORY and later calls allocate normally.
+ * after <= 0 disarms it. */
+void episdet_test_fail_allocation(int32_t after);
 
 /* Pairs search that allocates nothing -- no counterpart in the reference.
  * For callers that cannot let a library allocate device memory: a process

@@ -18,6 +18,14 @@
 #define EPISDET_COMPAT_SCORE EPISDET_SCORE_K2
 #endif
 
+// The reference's main prints C(numSNPs, k) through n_choose_k (declared at
+// include/helper.hpp:76, defined with its kernels at src/helper.cu:758-768).
+// A main linked against this shim without src/helper.cu finds it here; weak,
+// so a build that keeps src/helper.cu uses that one.
+__attribute__((weak)) unsigned long long n_choose_k(unsigned int n, unsigned int k) {
+    return (unsigned long long)episdet_n_choose_k(n, k);
+}
+
 cudaError_t EpistasisDetectionSearch(unsigned int* datasetCases, unsigned int* datasetControls, int numSNPs,
                                      int numCases, int numControls, unsigned int numSNPsWithPadding,
                                      int numCasesWithPadding, int numControlsWithPadding, int* roundsCounter,

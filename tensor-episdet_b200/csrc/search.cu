@@ -8,6 +8,7 @@
 // driver issues one persistent counting launch per first SNP (3-way) or one in
 // total (2-way), and synchronises once at the end.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
@@ -43,12 +44,20 @@ episdet_status cuda_fail(cudaError_t e, const char* what) {
     return set_error(EPISDET_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
+// Allocation-failure injection (episdet_test_fail_allocation): the number of
+// allocations still to make before one fails; 0 = disarmed.
+static std::atomic<int> g_fail_alloc{0};
+
 cudaError_t DevBuf::ensure(size_t bytes) {
     if (bytes <= cap && p) return cudaSuccess;
     if (p) cudaFree(p);
     p = nullptr;
     cap = 0;
     size_t want = std::max<size_t>(bytes, 256);
+    int left = g_fail_alloc.load();
+    while (left > 0 && !g_fail_alloc.compare_exchange_weak(left, left - 1)) {
+    }
+    if (left == 1) return cudaErrorMemoryAllocation;
     cudaError_t e = cudaMalloc(&p, want);
     if (e == cudaSuccess) cap = want;
     return e;
@@ -668,6 +677,8 @@ extern "C" episdet_status episdet_release_workspace(int32_t device) {
     }
     return EPISDET_OK;
 }
+
+extern "C" void episdet_test_fail_allocation(int32_t after) { episdet::g_fail_alloc.store(after > 0 ? after : 0); }
 
 extern "C" int32_t episdet_tuned_stage(int32_t order, int32_t score, int32_t num_cases, int32_t num_controls) {
     return episdet::tune_lookup(episdet::tune_key(order, score, num_cases, num_controls));

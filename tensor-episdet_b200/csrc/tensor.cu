@@ -68,7 +68,14 @@ constexpr int kThreads = 320;
 constexpr int kEpiThreads = 256;
 constexpr int kEpiPerStep = kEpiThreads * 2;
 static_assert(kMaxTopK + kEpiPerStep <= kCap, "candidate buffer too small for one step of offers");
-constexpr uint64_t kWaitLimitNs = 4000000000ull;
+// Waits for work (operand copies, MMA commits, the scoring warps) give up
+// after TcParams::wait_ns.  Drains before exit wait for the copies and MMAs
+// still in flight: up to kDrainLimitNs, or kAbortDrainNs once the CTA is
+// aborting (a copy the peer CTA never issued must not hold the drain up; the
+// pause before exit covers copies still landing).
+constexpr uint64_t kDrainLimitNs = 4000000000ull;
+constexpr uint64_t kAbortDrainNs = 2000000ull;
+constexpr uint64_t kAbortPauseNs = 200000ull;
 constexpr uint32_t kIdesc = ptx::idesc_u8(128);
 constexpr uint32_t kIdescPair = ptx::idesc_mxf4(kNPair, 256);  // CTA-pair e2m1 MMA, M = 256, N = 112
 // TMEM of the pair kernel: four 112-column count segments (triplets: one
@@ -123,7 +130,33 @@ struct TcParams {
     uint4* pair_out0;
     uint4* pair_out1;
     int* err;
+    uint64_t wait_ns;  // limit of every wait for work
+    const int* hold;   // failure-detection test: a word the scoring warps wait for (nothing sets it), or null
 };
+
+// Waits until *word != 0; false after limit_ns.
+__device__ __forceinline__ bool wait_word(const int* word, uint64_t limit_ns) {
+    const uint64_t t0 = ptx::globaltimer();
+    while (*(const volatile int*)word == 0) {
+        if (ptx::globaltimer() - t0 > limit_ns) return false;
+        __nanosleep(2000);
+    }
+    return true;
+}
+
+// Drain wait for copies or MMAs in flight: gives up after kDrainLimitNs, or
+// after kAbortDrainNs once *abort is set.
+__device__ __forceinline__ bool drain_wait(uint64_t* bar, uint32_t parity, volatile int* abort) {
+    if (ptx::mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = ptx::globaltimer();
+    for (uint32_t it = 1;; ++it) {
+        if (ptx::mbar_try_wait(bar, parity)) return true;
+        if ((it & 255) == 0) {
+            const uint64_t dt = ptx::globaltimer() - t0;
+            if (dt > kDrainLimitNs || (*abort && dt > kAbortDrainNs)) return false;
+        }
+    }
+}
 
 // Shared-memory layout of tc_kernel<PAIR, STAGE>.  A stage holds one K block of this
 // CTA's 128 A rows and of its B rows: all 128 for one CTA, 56 of the pair's
@@ -629,7 +662,7 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                 const int brow0 = PAIR ? tl.y * kNPair + rank * C::kBRows : tl.y * kTileRows;
                 for (int s = 0; ok && s < nseg; ++s) {
                     for (int kb = seg[s].kb0; kb < seg[s].kb1; ++kb) {
-                        if (!ptx::mbar_wait(&empty[stage], phase ^ 1, abort, kWaitLimitNs)) {
+                        if (!ptx::mbar_wait(&empty[stage], phase ^ 1, abort, P.wait_ns)) {
                             ok = false;
                             break;
                         }
@@ -657,17 +690,13 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
             if (!ok) {
                 record_error(P.err, 1);
                 *s_abort = 1;
-                // The odd CTA cannot observe its copies; give any still in
-                // flight time to land (they complete within microseconds).
-                if (PAIR && rank != 0 && issued) {
-                    const uint64_t t0 = ptx::globaltimer();
-                    while (ptx::globaltimer() - t0 < 200000ull) __nanosleep(1000);
-                }
             }
-            // Never leave with a copy in flight (the even CTA's barriers count both CTAs' copies).
+            (void)issued;
+            // Never leave with a copy in flight: the even CTA's barriers count
+            // both CTAs' copies; the odd CTA's copies of a stage the even CTA
+            // never armed land during the pause before exit (see the end).
             for (int i = 0; i < kStages; ++i)
-                if (pend[i] && !ptx::mbar_wait(&full[i], pend_phase[i], s_never, kWaitLimitNs))
-                    record_error(P.err, 2);
+                if (pend[i] && !drain_wait(&full[i], pend_phase[i], abort)) record_error(P.err, 2);
         }
     } else if (warp == 1) {
         // ---------------------------------------------------- MMA issuer
@@ -684,7 +713,7 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                 // Pair kernel: segment 0's columns are free once both CTAs'
                 // epilogues have copied out (or finished with) the previous tile's.
                 if constexpr (STAGE) {
-                    if (!ptx::mbar_wait_cluster(&tempty[1], (use & 1) ^ 1, abort, kWaitLimitNs)) {
+                    if (!ptx::mbar_wait_cluster(&tempty[1], (use & 1) ^ 1, abort, P.wait_ns)) {
                         ok = false;
                         break;
                     }
@@ -696,8 +725,8 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                 const uint32_t dbase = tmem + (uint32_t)(b * nseg * C::kNSeg);
                 for (int s = 0; ok && s < nseg; ++s) {
                     if (s == late_at) {
-                        const bool freed = PAIR ? ptx::mbar_wait_cluster(&tempty[b], (use & 1) ^ 1, abort, kWaitLimitNs)
-                                                : ptx::mbar_wait(&tempty[b], (use & 1) ^ 1, abort, kWaitLimitNs);
+                        const bool freed = PAIR ? ptx::mbar_wait_cluster(&tempty[b], (use & 1) ^ 1, abort, P.wait_ns)
+                                                : ptx::mbar_wait(&tempty[b], (use & 1) ^ 1, abort, P.wait_ns);
                         if (!freed) {
                             ok = false;
                             break;
@@ -706,7 +735,7 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                     }
                     const uint32_t dseg = dbase + (uint32_t)(s * C::kNSeg);
                     for (int kb = seg[s].kb0; kb < seg[s].kb1; ++kb) {
-                        if (!ptx::mbar_wait(&full[stage], phase, abort, kWaitLimitNs)) {
+                        if (!ptx::mbar_wait(&full[stage], phase, abort, P.wait_ns)) {
                             ok = false;
                             break;
                         }
@@ -748,8 +777,7 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                 ptx::mma_commit_pair_mc(drain, 0x1);
             else
                 ptx::mma_commit(drain);
-            if (!ptx::mbar_wait(drain, 0, s_never, kWaitLimitNs))
-                record_error(P.err, 4);
+            if (!ptx::mbar_wait(drain, 0, s_never, kDrainLimitNs)) record_error(P.err, 4);
         }
     } else {
         // ---------------------------------------------------- epilogue
@@ -784,7 +812,8 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
             // The decision to leave must be uniform over the 256 epilogue
             // threads (they meet at named barriers), so it is taken after a
             // barrier from a flag only they write.
-            if (!ptx::mbar_wait(&tfull[b], use & 1, abort, kWaitLimitNs)) *s_epi_fail = 1;
+            if (local == 0 && P.hold && !wait_word(P.hold, P.wait_ns)) *s_epi_fail = 1;
+            if (!*(volatile int*)s_epi_fail && !ptx::mbar_wait(&tfull[b], use & 1, abort, P.wait_ns)) *s_epi_fail = 1;
             bar();
             if (*(volatile int*)s_epi_fail) {
                 ok = false;
@@ -970,6 +999,17 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
         ptx::cluster_sync();
     else
         __syncthreads();
+    // After an abort, copies that no barrier of this CTA tracks (its half of a
+    // stage the peer never armed) complete within microseconds: pause before
+    // either CTA of the pair leaves.
+    if (threadIdx.x == 0 && *abort) {
+        const uint64_t t0 = ptx::globaltimer();
+        while (ptx::globaltimer() - t0 < kAbortPauseNs) __nanosleep(1000);
+    }
+    if constexpr (PAIR)
+        ptx::cluster_sync();
+    else
+        __syncthreads();
     if (warp == 1) {
         ptx::tc_fence_after();
         if constexpr (PAIR)
@@ -1059,6 +1099,8 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     p.first_begin = fb;
     p.first_end = fe;
     p.err = d_err;
+    p.wait_ns = (uint64_t)(o.wait_limit_ms > 0 ? o.wait_limit_ms : 4000) * 1000000ull;
+    p.hold = (o.flags & EPISDET_FLAG_INJECT_STALL) ? d_err + 3 : nullptr;
     const bool mi = T.score == EPISDET_SCORE_MI;
 
     if (o.order == 2) {

@@ -24,6 +24,7 @@ HOST, DEVICE = 0, 1
 ENGINE_AUTO, ENGINE_TENSOR, ENGINE_SIMT = 0, 1, 2
 FLAG_PROGRESS, FLAG_NO_VALIDATE, FLAG_TIMING = 0x1, 0x2, 0x4
 FLAG_AUTOTUNE = 0x8  # measure the triplet instance per shape and cache the choice
+FLAG_INJECT_STALL = 0x10  # testing aid: every tensor launch waits on a word nothing sets and times out
 
 STATUS = {
     0: "EPISDET_OK",
@@ -45,7 +46,7 @@ EXPORTED = [
     "episdet_generate", "episdet_generate_cohort", "episdet_generate_labels", "episdet_n_choose_k",
     "episdet_status_string", "episdet_last_error", "episdet_abi_version", "episdet_release_workspace",
     "episdet_search_pairs_noalloc", "episdet_binarize", "episdet_perm_pvalues", "episdet_search_resumable",
-    "episdet_tuned_stage",
+    "episdet_tuned_stage", "episdet_test_fail_allocation",
 ]
 
 
@@ -70,7 +71,7 @@ class Options(ctypes.Structure):
     _fields_ = [("order", ctypes.c_int32), ("score", ctypes.c_int32), ("top_k", ctypes.c_int32),
                 ("device", ctypes.c_int32), ("engine", ctypes.c_int32), ("first_begin", ctypes.c_int32),
                 ("first_end", ctypes.c_int32), ("flags", ctypes.c_uint32), ("stream", ctypes.c_uint64),
-                ("reserved", ctypes.c_int32 * 6)]
+                ("wait_limit_ms", ctypes.c_int32), ("reserved", ctypes.c_int32 * 5)]
 
 
 class Result(ctypes.Structure):
@@ -143,6 +144,8 @@ def lib() -> ctypes.CDLL:
     L.episdet_abi_version.restype = ctypes.c_int32
     L.episdet_release_workspace.argtypes = [ctypes.c_int32]
     L.episdet_release_workspace.restype = ctypes.c_int
+    L.episdet_test_fail_allocation.argtypes = [ctypes.c_int32]
+    L.episdet_test_fail_allocation.restype = None
     L.episdet_search_pairs_noalloc.argtypes = [P(Dataset), P(Options), P(Result)]
     L.episdet_search_pairs_noalloc.restype = ctypes.c_int
     _lib = L
@@ -289,7 +292,7 @@ def _ptr(a):
 
 
 def make_options(order=3, score="k2", top_k=1024, device=0, engine="auto", first_begin=0, first_end=0,
-                 flags=0, stream=0) -> Options:
+                 flags=0, stream=0, wait_limit_ms=0) -> Options:
     o = Options()
     lib().episdet_default_options(ctypes.byref(o))
     o.order = order
@@ -300,6 +303,7 @@ def make_options(order=3, score="k2", top_k=1024, device=0, engine="auto", first
         if isinstance(engine, str) else int(engine)
     o.first_begin, o.first_end, o.flags = first_begin, first_end, flags
     o.stream = int(stream)
+    o.wait_limit_ms = int(wait_limit_ms)
     return o
 
 
@@ -326,7 +330,7 @@ def _to_result(order: int, r: Result, bufs) -> SearchResult:
 
 def search(cases, controls, num_cases: int, num_controls: int, *, num_snps: Optional[int] = None, order: int = 3,
            score="k2", top_k: int = 1024, device: int = 0, engine="auto", first_begin: int = 0, first_end: int = 0,
-           flags: int = 0, stream: int = 0) -> SearchResult:
+           flags: int = 0, stream: int = 0, wait_limit_ms: int = 0) -> SearchResult:
     """Exhaustive search; cases/controls are host uint32 arrays or CUDA tensors in the plane format."""
     pc, mc = _ptr(cases)
     pn, mn = _ptr(controls)
@@ -334,7 +338,7 @@ def search(cases, controls, num_cases: int, num_controls: int, *, num_snps: Opti
         raise TypeError("cases and controls must live in the same memory")
     M = num_snps if num_snps is not None else int(cases.shape[0])
     d = Dataset(pc, pn, M, num_cases, num_controls, mc)
-    o = make_options(order, score, top_k, device, engine, first_begin, first_end, flags, stream)
+    o = make_options(order, score, top_k, device, engine, first_begin, first_end, flags, stream, wait_limit_ms)
     r, bufs = _result_buffers(top_k)
     _check(lib().episdet_search(ctypes.byref(d), ctypes.byref(o), ctypes.byref(r)))
     return _to_result(order, r, bufs)
@@ -361,6 +365,16 @@ def search_resumable(cases, controls, num_cases: int, num_controls: int, checkpo
     r, bufs = _result_buffers(top_k)
     _check(lib().episdet_search_resumable(ctypes.byref(d), ctypes.byref(o), ctypes.byref(rs), ctypes.byref(r)))
     return _to_result(order, r, bufs), bool(rs.done), int(rs.next_first)
+
+
+def release_workspace(device: int = 0) -> None:
+    _check(lib().episdet_release_workspace(device))
+
+
+def test_fail_allocation(after: int) -> None:
+    """Testing aid: the after-th device allocation from now on fails once as
+    out of memory (after <= 0 disarms)."""
+    lib().episdet_test_fail_allocation(after)
 
 
 def tuned_stage(order: int, score, num_cases: int, num_controls: int) -> int:

@@ -32,6 +32,28 @@ def test_noalloc_matches_search_twice(episdet):
             assert r.sets_evaluated == ref.sets_evaluated
 
 
+@pytest.mark.parametrize("M,nc,nn,k,fb,fe", [(300, 2100, 1900, 128, 37, 100), (4096, 60000, 71072, 1024, 0, 0),
+                                              (1000, 1, 131071, 1024, 990, 999)],
+                         ids=["slab", "at-every-limit", "one-case"])
+def test_noalloc_slabs_and_limits(episdet, M, nc, nn, k, fb, fe):
+    """A first-SNP slab, and a search at the documented limits (4096 SNPs,
+    131,072 samples, top_k 1024), which fill the fixed regions of the array to
+    capacity, against the ordinary entry point."""
+    import torch
+
+    cases, controls = episdet.generate(0xA110C + M, M, nc, nn)
+    dc = torch.from_numpy(cases.view(np.int32)).cuda()
+    dn = torch.from_numpy(controls.view(np.int32)).cuda()
+    ref = episdet.search(cases, controls, nc, nn, order=2, top_k=k, first_begin=fb, first_end=fe)
+    for _ in range(2):
+        r = episdet.search_pairs_noalloc(dc, dn, nc, nn, num_snps=M, top_k=k, first_begin=fb, first_end=fe)
+        assert r.snps == ref.snps and r.score == ref.score
+        assert np.array_equal(r.top_snps, ref.top_snps)
+        assert np.array_equal(r.top_fp32.view(np.uint32), ref.top_fp32.view(np.uint32))
+        assert np.array_equal(r.top_fp64, ref.top_fp64)
+        assert r.sets_evaluated == ref.sets_evaluated
+
+
 def test_noalloc_rejects_oversize_and_host_inputs(episdet):
     import torch
 
