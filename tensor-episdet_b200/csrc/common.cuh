@@ -66,6 +66,9 @@ struct ScoreTables {
     double inv_n64;
     double hy64;
     int score;          // 0 = K2, 1 = MI
+    // K2 only: a bound on |FP32 score - k2_approx32 score| over every valid
+    // table of this sample count (the scoring filter of the triplet engine).
+    float k2_margin;
 };
 
 // The FP32 table's first kLoTab entries are also staged in shared memory by
@@ -104,6 +107,43 @@ __device__ __forceinline__ float score32_lut(const ScoreTables& T, const Lut& lu
         hx = __fmaf_rn(-__fadd_rn(pc, pn), lut(cs[c] + cn[c]), hx);
     }
     return __fsub_rn(__fadd_rn(hx, T.hy32), ha);
+}
+
+// ------------------------------------------------- K2 scoring filter
+// lnGamma(v + 1) without a table: the exact FP32 table value for v <
+// kSmallTab (from a 32-entry shared-memory copy, one entry per bank, so any
+// gather is conflict-free) and above it Stirling's series cut after its
+// constant term, (z - 1/2) ln z - z + ln(2 pi) / 2 with z = v + 1 (the next
+// term, 1/(12 z), is below 0.0026 there), in FP32 with the hardware log2.
+// Every step is an explicit round-to-nearest operation, so the value of a
+// given v is the same wherever it is evaluated; the largest distance to the
+// FP32 table over 0 <= v <= N + 1 is measured once per sample count
+// (k2_filter_margin) and the filter's bound is built from it.
+constexpr int kSmallTab = 32;
+constexpr float kLn2f = 0.693147182464599609375f;      // ln 2 rounded to float
+constexpr float kHalfLn2Pif = 0.918938517570495605469f;  // ln(2 pi) / 2 rounded to float
+
+__device__ __forceinline__ float lngamma1_stirling(int v) {
+    const float z = __int2float_rn(v + 1);
+    const float lnz = __fmul_rn(__log2f(z), kLn2f);
+    return __fmaf_rn(__fsub_rn(z, 0.5f), lnz, __fsub_rn(kHalfLn2Pif, z));
+}
+
+__device__ __forceinline__ float lngamma1_filter(const float* s_small, int v) {
+    return v < kSmallTab ? s_small[v] : lngamma1_stirling(v);
+}
+
+// The K2 score of one table with lngamma1_filter in place of the table, in
+// the cell order and operation sequence of score32_lut.  Its distance to the
+// exact FP32 score is at most ScoreTables::k2_margin.
+template <int NC>
+__device__ __forceinline__ float k2_approx32(const float* s_small, const int* cs, const int* cn) {
+    float s = 0.0f;
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+        s = __fadd_rn(s, __fsub_rn(__fadd_rn(lngamma1_filter(s_small, cn[c]), lngamma1_filter(s_small, cs[c])),
+                                   lngamma1_filter(s_small, cn[c] + cs[c] + 1)));
+    return fabsf(s);
 }
 
 template <int NC>
@@ -195,6 +235,7 @@ struct LocalTopK {
     Cand* thr;     // shared scalar
     int k;
     int tid;
+    uint32_t* gkey = nullptr;  // optional: search-wide smallest k-th key (Slots::gkey)
 
     // `hi` is this thread's highest slot + 1 since the last compaction.  The
     // atomic hands slots out in order, so the largest `hi` over the threads is
@@ -219,17 +260,20 @@ struct LocalTopK {
         }
     }
 
-    // Bitonic sort of buf[0..CAP) with entries >= n set to worst; requires a
-    // barrier functor covering exactly the NT participating threads, and every
-    // offer of those threads must be ordered before the call by a barrier.
+    // Bitonic sort of buf[0..P), P the power of two >= n (at most CAP), with
+    // entries >= n set to worst; requires a barrier functor covering exactly
+    // the NT participating threads, and every offer of those threads must be
+    // ordered before the call by a barrier (so every thread reads the same n).
     template <class Bar>
     __device__ void compact(Bar bar) const {
         int n = *count;
-        for (int i = n + tid; i < CAP; i += NT) buf[i] = cand_worst();
+        int P = 2;
+        while (P < n) P <<= 1;
+        for (int i = n + tid; i < P; i += NT) buf[i] = cand_worst();
         bar();
-        for (int kk = 2; kk <= CAP; kk <<= 1) {
+        for (int kk = 2; kk <= P; kk <<= 1) {
             for (int j = kk >> 1; j > 0; j >>= 1) {
-                for (int i = tid; i < CAP; i += NT) {
+                for (int i = tid; i < P; i += NT) {
                     int ixj = i ^ j;
                     if (ixj > i) {
                         Cand a = buf[i], b = buf[ixj];
@@ -247,6 +291,7 @@ struct LocalTopK {
             int m = n < k ? n : k;
             *count = m;
             *thr = (m >= k) ? buf[k - 1] : cand_worst();
+            if (gkey && m >= k) atomicMin(gkey, buf[k - 1].key);
         }
         bar();
     }
@@ -257,6 +302,7 @@ struct LocalTopK {
         if (tid == 0) {
             *count = slot_count;
             *thr = (slot_count >= k) ? slot[k - 1] : cand_worst();
+            if (gkey && slot_count >= k) atomicMin(gkey, slot[k - 1].key);
         }
         bar();
     }

@@ -22,6 +22,10 @@ struct Slots {
     int* counts;     // [nslots]
     int nslots;
     int k;
+    // The smallest k-th best key any CTA has held in this search (0xFFFFFFFF
+    // until one held k candidates): a set whose key is larger has k better
+    // sets and cannot be in the search's top k.
+    uint32_t* gkey;
 };
 
 __device__ __forceinline__ void load_marg3(const int* m, int M, int snp, int out[3]) {

@@ -228,6 +228,7 @@ static episdet_status search_locked(const episdet_dataset* data, const episdet_o
     slots.counts = (int*)(S + kOffCounts);
     slots.nslots = grid;
     slots.k = o.top_k;
+    slots.gkey = nullptr;
     CUDA_TRY(cudaMemsetAsync(slots.counts, 0, sizeof(int) * grid, stream));
     search2_simt_kernel<<<grid, kSimtBlockThreads, kSimtSmem2, stream>>>(D, T, (const int2*)(S + kOffTiles), ntiles,
                                                                           fb, fe, slots, 0, nullptr, nullptr);

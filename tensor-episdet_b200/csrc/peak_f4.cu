@@ -632,6 +632,12 @@ static int sweep(int sms, int units, unsigned long long* d_cyc) {
         rc |= sweep_point<224, true>(sms, units, c, 64, 0, 1, d_cyc);
         rc |= sweep_point<256, true>(sms, units, c, 64, 0, 1, d_cyc);
     }
+    // The instruction's asymptotic rate: long commit groups (a commit every
+    // 32 and 64 MMAs), the form the roofline of the engine is quoted against.
+    for (int c = 32; c <= 64; c *= 2) {
+        rc |= sweep_point<112, true>(sms, units, c, 128, 0, 1, d_cyc);
+        rc |= sweep_point<256, true>(sms, units, c, 128, 0, 1, d_cyc);
+    }
     const int inf[3] = {32, 128, 256};
     for (int f : inf) rc |= sweep_point<112, true>(sms, units, 4, f, 0, 1, d_cyc);
     rc |= sweep_point<112, true>(sms, units, 16, 64, 4, 1, d_cyc);

@@ -181,6 +181,11 @@ episdet_status build_tables(Workspace* w, int score, int nc, int nn, ScoreTables
         CUDA_TRY(cudaMemcpyAsync(w->t64.p, t64.data(), sizeof(double) * size, cudaMemcpyHostToDevice, w->st));
         CUDA_TRY(cudaStreamSynchronize(w->st));
         w->h2d += (int64_t)size * (sizeof(float) + sizeof(double));
+        w->k2_margin = 0.0f;
+        if (score == EPISDET_SCORE_K2) {
+            episdet_status st = k2_filter_margin(w, nc, nn, (const float*)w->t32.p, &w->k2_margin);
+            if (st != EPISDET_OK) return st;
+        }
         w->tab_score = score;
         w->tab_nc = nc;
         w->tab_nn = nn;
@@ -192,6 +197,7 @@ episdet_status build_tables(Workspace* w, int score, int nc, int nn, ScoreTables
     T->hy32 = w->hy32;
     T->hy64 = w->hy64;
     T->score = score;
+    T->k2_margin = w->k2_margin;
     return EPISDET_OK;
 }
 
@@ -259,12 +265,14 @@ episdet_status stage_dataset(Workspace* w, const episdet_dataset* d, bool valida
 
 episdet_status prepare_slots(Workspace* w, int nslots, int k, Slots* S) {
     CUDA_TRY(w->slots.ensure(sizeof(Cand) * (size_t)nslots * k));
-    CUDA_TRY(w->counts.ensure(sizeof(int) * (size_t)nslots));
+    CUDA_TRY(w->counts.ensure(sizeof(int) * ((size_t)nslots + 1)));
     CUDA_TRY(cudaMemsetAsync(w->counts.p, 0, sizeof(int) * (size_t)nslots, w->st));
+    CUDA_TRY(cudaMemsetAsync((int*)w->counts.p + nslots, 0xFF, sizeof(int), w->st));
     S->lists = (Cand*)w->slots.p;
     S->counts = (int*)w->counts.p;
     S->nslots = nslots;
     S->k = k;
+    S->gkey = (uint32_t*)((int*)w->counts.p + nslots);
     return EPISDET_OK;
 }
 

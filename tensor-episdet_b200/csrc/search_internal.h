@@ -52,6 +52,7 @@ struct Workspace {
     DevBuf xsub[8];       // per-X sample-regrouped operand rows (tensor engine)
     DevBuf xinfo;         // per-X segment tables (tensor engine)
     DevBuf tensor_flag;   // device error / progress words of the tensor engine
+    DevBuf cbuf;          // per-CTA candidate buffers of the filtered triplet kernel
     DevBuf perm_planes, perm_cls[2], perm_idx;  // phenotype-permutation staging
     DevBuf bin_geno, bin_idx, bin_out[2];       // genotype-matrix binarizer staging
     // Per-call accounting.
@@ -63,14 +64,14 @@ struct Workspace {
     double executed_macs = 0.0;
     int tab_score = -1, tab_nc = -1, tab_nn = -1;
     int stage_override = -1;  // triplet instance: -1 by the class-size rule, 0 plain, 1 staged
-    float inv32 = 0.0f, hy32 = 0.0f;
+    float inv32 = 0.0f, hy32 = 0.0f, k2_margin = 0.0f;
     double inv64 = 0.0, hy64 = 0.0;
 
     void release_all() {
         DevBuf* all[] = {&bits[0], &bits[1], &marg[0], &marg[1], &pair4[0], &pair4[1], &t32, &t64, &slots,
                          &counts, &tiles, &merged, &mcount, &fp64, &flag, &planes8, &xsub[0], &xsub[1], &xsub[2], &xsub[3], &xsub[4], &xsub[5],
                          &xsub[6], &xsub[7], &xinfo,
-                         &tensor_flag, &perm_planes, &perm_cls[0], &perm_cls[1], &perm_idx,
+                         &tensor_flag, &cbuf, &perm_planes, &perm_cls[0], &perm_cls[1], &perm_idx,
                          &bin_geno, &bin_idx, &bin_out[0], &bin_out[1]};
         for (DevBuf* b : all) b->release();
         tab_score = tab_nc = tab_nn = -1;
@@ -103,6 +104,10 @@ void begin_call(Workspace* w, const episdet_options& o);
 // One search; the caller holds w->mu and has validated the options.
 episdet_status search_locked(Workspace* w, const episdet_dataset* data, const episdet_options& o,
                              episdet_result* result);
+
+// Bound of the K2 scoring filter for a sample count (tensor.cu): measures the
+// filter's largest distance to the FP32 table d_t32 on the device.
+episdet_status k2_filter_margin(Workspace* w, int nc, int nn, const float* d_t32, float* margin);
 
 // Sets the tensor engine's kernel attributes on the current device.
 episdet_status tensor_init_attributes();

@@ -36,6 +36,9 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
 #include <cstdio>
 #include <vector>
 
@@ -68,6 +71,15 @@ constexpr int kThreads = 320;
 constexpr int kEpiThreads = 256;
 constexpr int kEpiPerStep = kEpiThreads * 2;
 static_assert(kMaxTopK + kEpiPerStep <= kCap, "candidate buffer too small for one step of offers");
+// The filtered K2 triplet instances keep their candidate buffer in global
+// memory and check its fill once per tile: room for k plus a whole tile's
+// offers (each epilogue thread scores 2 sets in each of its 7 chunks).
+constexpr int kCapG = 8192;
+// Filtered K2 triplet instances: operand K blocks prefetched into L2 this far
+// ahead of the stage loads.
+constexpr int kPrefetchKb = 8;
+constexpr int kEpiPerTile = kEpiThreads * 2 * (kNPair / 16);
+static_assert(kMaxTopK + kEpiPerTile <= kCapG, "global candidate buffer too small for one tile of offers");
 // Waits for work (operand copies, MMA commits, the scoring warps) give up
 // after TcParams::wait_ns.  Drains before exit wait for the copies and MMAs
 // still in flight: up to kDrainLimitNs, or kAbortDrainNs once the CTA is
@@ -130,6 +142,7 @@ struct TcParams {
     uint4* pair_out0;
     uint4* pair_out1;
     int* err;
+    Cand* cbuf;        // kFeatGlobalCands instances: [grid][kCapG] candidate buffers in global memory
     uint64_t wait_ns;  // limit of every wait for work
     const int* hold;   // failure-detection test: a word the scoring warps wait for (nothing sets it), or null
 };
@@ -158,32 +171,67 @@ __device__ __forceinline__ bool drain_wait(uint64_t* bar, uint32_t parity, volat
     }
 }
 
-// Shared-memory layout of tc_kernel<PAIR, STAGE>.  A stage holds one K block of this
-// CTA's 128 A rows and of its B rows: all 128 for one CTA, 56 of the pair's
-// 112 for a CTA pair (PAIR), where the other CTA of the pair holds the rest.
-template <bool PAIR, bool STAGE = false>
+// Features of a kernel instance (a bit mask):
+//   kFeatFilter       K2 scoring filter (k2_approx32); only a 32-entry table in
+//                     shared memory;
+//   kFeatBigStages    stages of two K blocks (one MMA commit per 8 MMAs: a
+//                     commit costs the tensor pipe about as much as four MMAs
+//                     of this shape, profiles/tcgen05_mma_peak.md), three of them;
+//   kFeatGlobalCands  candidate buffer in a global per-CTA region, its fill
+//                     checked once per tile;
+//   kFeatOpPrefetch   operand K blocks prefetched into L2 ahead of the stage loads;
+//   kFeatPairPrefetch the Y-Z and X-Z pair-table rows of a tile prefetched into
+//                     L2 while its MMAs run.
+enum : int { kFeatFilter = 1, kFeatBigStages = 2, kFeatGlobalCands = 4, kFeatOpPrefetch = 8, kFeatPairPrefetch = 16 };
+
+// Shared-memory layout of tc_kernel<PAIR, STAGE, FEAT>.  A K block holds
+// 128 bytes of this CTA's 128 A rows and of its B rows: all 128 for one CTA,
+// 56 of the pair's 112 for a CTA pair (PAIR), where the other CTA of the pair
+// holds the rest.  A stage holds kKbPerStage K blocks and is released by one
+// MMA commit.
+template <bool PAIR, bool STAGE = false, int FEAT = 0>
 struct Cfg {
-    // Four stages: a fifth would push the staged instance past the 196 KB
-    // carve-out, halving the L1 left for the epilogue's global table reads.
-    static constexpr int kStages = 4;
+    static constexpr bool FILTER = (FEAT & kFeatFilter) != 0;
+    static constexpr bool GCANDS = (FEAT & kFeatGlobalCands) != 0;
+    static constexpr int kKbPerStage = (FEAT & kFeatBigStages) ? 2 : 1;
+    static constexpr int kStages = (FEAT & kFeatBigStages) ? 3 : 4;
     static constexpr int kBRows = PAIR ? kZSnpsPair : 128;
     static constexpr int kNSeg = PAIR ? kNPair : 128;      // accumulator columns per count segment
     static constexpr int kZSnps = PAIR ? kZSnpsPair : kTileSnps;  // B SNPs per tile
     static constexpr int kChunks = kNSeg / 16;              // 8-column chunks per epilogue warp
-    static constexpr int kStageBytes = kTileBytes + kBRows * kKB;
+    static constexpr int kKbBytes = kTileBytes + kBRows * kKB;  // A then B of one K block
+    static constexpr int kStageBytes = kKbPerStage * kKbBytes;
     static constexpr size_t kSmemTopk = (size_t)kStages * kStageBytes;
-    static constexpr size_t kSmemLo = kSmemTopk + (size_t)kCap * sizeof(Cand);  // [kLoTab] float
+    // FP32 score table entries kept in shared memory: kSmallTab (the filter's)
+    // or kLoTab (exact scoring of every set).
+    static constexpr int kLoEntries = FILTER ? kSmallTab : kLoTab;
+    // The candidate buffer: in shared memory, or (GCANDS) in a global per-CTA
+    // region, leaving the shared memory to the stages and to L1.
+    static constexpr size_t kSmemLo = kSmemTopk + (GCANDS ? 0 : (size_t)kCap * sizeof(Cand));
     // STAGE: count segment 0 of the tile copied out of TMEM as 16-bit counts,
     // [epilogue thread][chunk] x 8 columns.
-    static constexpr size_t kSmemStage = kSmemLo + (size_t)kLoTab * sizeof(float);
+    static constexpr size_t kSmemStage = kSmemLo + (size_t)kLoEntries * sizeof(float);
     static constexpr size_t kSmemBars = kSmemStage + (STAGE ? (size_t)kEpiThreads * kChunks * sizeof(uint4) : 0);
     static constexpr int kNumBars = 2 * kStages + 5;  // full, empty, tfull[2], tempty[2], drain
     static constexpr size_t kSmemMisc = kSmemBars + ((kNumBars * sizeof(uint64_t) + 63) & ~size_t(63));
     static constexpr size_t kSmemGroup = kSmemMisc + 64;
     static constexpr size_t kSmemTotal = kSmemGroup + 256 + 1024;
     static_assert(kSmemTotal <= 232448, "tc_kernel shared memory exceeds 227 KB");
-    static_assert(kStageBytes % 1024 == 0, "operand tiles must stay 1024-byte aligned");
+    static_assert(kKbBytes % 1024 == 0 && kTileBytes % 1024 == 0, "operand tiles must stay 1024-byte aligned");
 };
+
+// The configuration of one kernel instance, used by the kernel and by every
+// host-side launch and attribute, so the two can never disagree on the layout.
+// The K2 triplet instances (the headline search) filter, run stages of two K
+// blocks, keep their candidates in global memory and prefetch their pair-table
+// rows; operand prefetch (kFeatOpPrefetch) measured slower and is off.  The MI
+// triplet, 2-way and pair-table instances keep the plain layout (with MI's
+// exact scoring, larger stages cost the epilogue more L1 than they gained).
+template <bool PAIR, bool TWO, int SC>
+constexpr int kInstanceFeat =
+    (PAIR && !TWO && SC == 0) ? (kFeatFilter | kFeatBigStages | kFeatGlobalCands | kFeatPairPrefetch) : 0;
+template <bool PAIR, bool STAGE, int SC = -1, bool TWO = false>
+using KCfg = Cfg<PAIR, STAGE, kInstanceFeat<PAIR, TWO, SC>>;
 
 // Per-launch copy of each group member's segments in shared memory.
 struct GroupSm {
@@ -525,18 +573,39 @@ __device__ __forceinline__ void record_error(int* err, int code) { atomicCAS(err
 // SC: the score fixed at compile time (0 = K2, 1 = MI) or -1 (read at run time).
 // TWO: the pair kernel scoring pairs (two class segments, two accumulator sets)
 // instead of counting triplets.
+// FILTER (the K2 triplet instances): each set's K2 score is first bounded
+// without table reads (k2_approx32); only sets that may be better than the
+// CTA's current k-th candidate are scored exactly (from the global table),
+// so the candidate lists are those of scoring every set.
 template <bool PAIR, bool STAGE, int SC = -1, bool TWO = false>
 __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
     tc_kernel(const __grid_constant__ TmapPack tm, const __grid_constant__ TcParams P) {
     static_assert(PAIR || !STAGE, "staging is a pair-kernel mode");
     static_assert(!TWO || (PAIR && !STAGE), "the 2-way pair kernel is the plain pair instance");
-    using C = Cfg<PAIR, STAGE>;
+    using C = KCfg<PAIR, STAGE, SC, TWO>;
+    constexpr bool FILTER = C::FILTER;
+    constexpr bool GCANDS = C::GCANDS;
+    constexpr bool OPF = (kInstanceFeat<PAIR, TWO, SC> & kFeatOpPrefetch) != 0;
+    constexpr bool PPF = (kInstanceFeat<PAIR, TWO, SC> & kFeatPairPrefetch) != 0;
     constexpr int kStages = C::kStages;
     constexpr int kStageBytes = C::kStageBytes;
+    constexpr int kKbBytes = C::kKbBytes;
+    constexpr int kKbPer = C::kKbPerStage;
     extern __shared__ uint8_t smem_raw[];
+    // A launch with less dynamic shared memory than this instance's layout
+    // needs is refused before anything touches it (uniform over the CTA and
+    // the pair, so no barrier is left waiting).
+    {
+        uint32_t dyn;
+        asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+        if (dyn < (uint32_t)C::kSmemTotal) {
+            if (threadIdx.x == 0) record_error(P.err, 7);
+            return;
+        }
+    }
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* stages = smem;
-    Cand* tbuf = reinterpret_cast<Cand*>(smem + C::kSmemTopk);
+    Cand* tbuf = GCANDS ? P.cbuf + (size_t)blockIdx.x * kCapG : reinterpret_cast<Cand*>(smem + C::kSmemTopk);
     float* s_lo = reinterpret_cast<float*>(smem + C::kSmemLo);
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + C::kSmemBars);
     uint64_t* full = bars;
@@ -661,21 +730,45 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                 const int arow0 = PAIR ? tl.x * 2 * kTileRows + rank * kTileRows : tl.x * kTileRows;
                 const int brow0 = PAIR ? tl.y * kNPair + rank * C::kBRows : tl.y * kTileRows;
                 for (int s = 0; ok && s < nseg; ++s) {
-                    for (int kb = seg[s].kb0; kb < seg[s].kb1; ++kb) {
+                    for (int kb = seg[s].kb0; kb < seg[s].kb1; kb += kKbPer) {
+                        // A stage holds up to kKbPer K blocks of one segment.
+                        const int nkb = min(kKbPer, seg[s].kb1 - kb);
                         if (!ptx::mbar_wait(&empty[stage], phase ^ 1, abort, P.wait_ns)) {
                             ok = false;
                             break;
                         }
                         uint8_t* sa = stages + (size_t)stage * kStageBytes;
+                        if constexpr (OPF) {
+                            // The K blocks kPrefetchKb ahead (same segment) into
+                            // L2, so that stage loads rarely wait for DRAM.
+#pragma unroll
+                            for (int j = 0; j < kKbPer; ++j) {
+                                const int pk = kb + j + kPrefetchKb;
+                                if (j < nkb && pk < seg[s].kb1) {
+                                    ptx::tma_prefetch_2d(tmap, pk * kKB, arow0);
+                                    ptx::tma_prefetch_2d(tmapb, pk * kKB, brow0);
+                                }
+                            }
+                        }
                         if constexpr (PAIR) {
-                            if (rank == 0) ptx::mbar_arrive_expect_tx(&full[stage], 2 * kStageBytes);
+                            if (rank == 0) ptx::mbar_arrive_expect_tx(&full[stage], (uint32_t)(2 * nkb * kKbBytes));
                             const uint32_t fb = full0 + (uint32_t)(stage * sizeof(uint64_t));
-                            ptx::tma_load_2d_pair(sa, tmap, kb * kKB, arow0, fb);
-                            ptx::tma_load_2d_pair(sa + kTileBytes, tmapb, kb * kKB, brow0, fb);
+#pragma unroll
+                            for (int j = 0; j < kKbPer; ++j)
+                                if (j < nkb) {
+                                    ptx::tma_load_2d_pair(sa + j * kKbBytes, tmap, (kb + j) * kKB, arow0, fb);
+                                    ptx::tma_load_2d_pair(sa + j * kKbBytes + kTileBytes, tmapb, (kb + j) * kKB, brow0,
+                                                          fb);
+                                }
                         } else {
-                            ptx::mbar_arrive_expect_tx(&full[stage], kStageBytes);
-                            ptx::tma_load_2d(sa, tmap, kb * kKB, arow0, &full[stage]);
-                            ptx::tma_load_2d(sa + kTileBytes, tmapb, kb * kKB, brow0, &full[stage]);
+                            ptx::mbar_arrive_expect_tx(&full[stage], (uint32_t)(nkb * kKbBytes));
+#pragma unroll
+                            for (int j = 0; j < kKbPer; ++j)
+                                if (j < nkb) {
+                                    ptx::tma_load_2d(sa + j * kKbBytes, tmap, (kb + j) * kKB, arow0, &full[stage]);
+                                    ptx::tma_load_2d(sa + j * kKbBytes + kTileBytes, tmapb, (kb + j) * kKB, brow0,
+                                                     &full[stage]);
+                                }
                         }
                         issued = true;
                         pend[stage] = !PAIR || rank == 0;  // completions land on the even CTA's barriers
@@ -734,22 +827,27 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                         ptx::tc_fence_after();
                     }
                     const uint32_t dseg = dbase + (uint32_t)(s * C::kNSeg);
-                    for (int kb = seg[s].kb0; kb < seg[s].kb1; ++kb) {
+                    for (int kb = seg[s].kb0; kb < seg[s].kb1; kb += kKbPer) {
+                        const int nkb = min(kKbPer, seg[s].kb1 - kb);
                         if (!ptx::mbar_wait(&full[stage], phase, abort, P.wait_ns)) {
                             ok = false;
                             break;
                         }
                         ptx::tc_fence_after();
-                        const uint32_t sa = ptx::smem_u32(stages + (size_t)stage * kStageBytes);
-                        const uint64_t ad = ptx::smem_desc_sw128(sa), bd = ptx::smem_desc_sw128(sa + kTileBytes);
 #pragma unroll
-                        for (int kk = 0; kk < kKB / 32; ++kk) {
-                            const uint32_t acc = (kb > seg[s].kb0 || kk > 0) ? 1u : 0u;
-                            if constexpr (PAIR)
-                                ptx::mma_mxf4_pair(dseg, ad + 2 * kk, bd + 2 * kk, kIdescPair, tmem + kSfCol,
-                                                   tmem + kSfCol + 32, acc);
-                            else
-                                ptx::mma_u8(dseg, ad + 2 * kk, bd + 2 * kk, kIdesc, acc);
+                        for (int j = 0; j < kKbPer; ++j) {
+                            if (j >= nkb) break;
+                            const uint32_t sa = ptx::smem_u32(stages + (size_t)stage * kStageBytes + j * kKbBytes);
+                            const uint64_t ad = ptx::smem_desc_sw128(sa), bd = ptx::smem_desc_sw128(sa + kTileBytes);
+#pragma unroll
+                            for (int kk = 0; kk < kKB / 32; ++kk) {
+                                const uint32_t acc = (kb + j > seg[s].kb0 || kk > 0) ? 1u : 0u;
+                                if constexpr (PAIR)
+                                    ptx::mma_mxf4_pair(dseg, ad + 2 * kk, bd + 2 * kk, kIdescPair, tmem + kSfCol,
+                                                       tmem + kSfCol + 32, acc);
+                                else
+                                    ptx::mma_u8(dseg, ad + 2 * kk, bd + 2 * kk, kIdesc, acc);
+                            }
                         }
                         if constexpr (PAIR)
                             ptx::mma_commit_pair_mc(&empty[stage], 0x3);  // frees the stage in both CTAs
@@ -790,7 +888,7 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
         const BarNamed bar{1, kEpiThreads};
         const bool maximize = SC >= 0 ? SC == 1 : P.T.score == 1;
         const int M = P.D.M;
-        LocalTopK<kCap, kEpiThreads> tk{tbuf, s_count, s_thr, P.S.k, etid};
+        LocalTopK<GCANDS ? kCapG : kCap, kEpiThreads> tk{tbuf, s_count, s_thr, P.S.k, etid, P.S.gkey};
         // The candidate buffer takes at most kEpiPerStep offers per chunk; its
         // fill is checked after every chunk.  (Checking less often would need
         // that many more free slots, i.e. a lower fill limit and more sorts.)
@@ -798,7 +896,7 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
         const LutShared lut{s_lo, P.T.t32};
         if (mode != kPairsStore) {
             // Low end of the FP32 table (every index the scorer can read is < N + 2).
-            const int nlo = min(P.D.n[0] + P.D.n[1] + 2, kLoTab);
+            const int nlo = min(P.D.n[0] + P.D.n[1] + 2, C::kLoEntries);
             for (int i = etid; i < nlo; i += kEpiThreads) s_lo[i] = __ldg(P.T.t32 + i);
             tk.load(P.S.lists + (size_t)blockIdx.x * P.S.k, P.S.counts[blockIdx.x], bar);
         }
@@ -809,6 +907,18 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
             const uint32_t use = (uint32_t)(local / nbuf);
             const int g = group_of(P, t);
             const int2 tl = P.grp[g].tiles[t - P.grp[g].cum];
+            if constexpr (PPF) {
+                // While this tile's MMAs run, bring its Y-Z and X-Z pair-table
+                // rows into L2 (one row of 56 entries per thread and class).
+                const int bz0 = tl.y * C::kZSnps;
+                const int nz = min(C::kZSnps, M - bz0);
+                if (nz > 0 && etid < 2 * kTileSnps + 2) {
+                    const int c = etid < 2 * kTileSnps ? etid / kTileSnps : etid - 2 * kTileSnps;
+                    const int row = etid < 2 * kTileSnps ? tl.x * 2 * kTileSnps + rank * kTileSnps + etid % kTileSnps
+                                                         : s_grp[g].x;
+                    if (row < M) ptx::prefetch_l2(P.D.pair4[c] + (size_t)row * M + bz0, (uint32_t)nz * 16u);
+                }
+            }
             // The decision to leave must be uniform over the 256 epilogue
             // threads (they meet at named barriers), so it is taken after a
             // barrier from a flag only they write.
@@ -911,6 +1021,12 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                     for (int e = 0; e < 4; ++e)
                         r[s][e] = __shfl_xor_sync(0xFFFFFFFFu, j_own ? v[s][e] : v[s][4 + e], 1);
                 Cand thr = *s_thr;
+                // FILTER: the smaller of this CTA's and the search-wide k-th
+                // best FP32 score so far (+inf until some CTA held k candidates).
+                uint32_t thr_key = thr.key;
+                if constexpr (FILTER) thr_key = min(thr_key, *(volatile uint32_t*)P.S.gkey);
+                const float thr_s = thr_key == 0xFFFFFFFFu ? __int_as_float(0x7F800000) : key_score(thr_key, false);
+                (void)thr_s;
 #pragma unroll
                 for (int z = 0; z < 2; ++z) {
                     const int bsnp = tl.y * C::kZSnps + ch * 4 + zoff + z;
@@ -975,15 +1091,24 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                         pair9_from4(yz9, yz, ma[c], mz);
                         derive27(tab[c], xy9[c], xz9, yz9);
                     }
-                    float sc = score32_lut<27, LutShared, SC>(P.T, lut, tab[0], tab[1]);
+                    float sc;
+                    if constexpr (FILTER) {
+                        // Provably worse than the k-th candidate: not offered,
+                        // as exact scoring would not have offered it either.
+                        if (__fadd_rn(thr_s, P.T.k2_margin) < k2_approx32<27>(s_lo, tab[0], tab[1])) continue;
+                        sc = score32_lut<27, LutGlobal, 0>(P.T, LutGlobal{P.T.t32}, tab[0], tab[1]);
+                    } else {
+                        sc = score32_lut<27, LutShared, SC>(P.T, lut, tab[0], tab[1]);
+                    }
                     Cand cd;
                     cd.key = score_key(sc, maximize);
                     cd.pad = 0;
                     cd.set = set_key3((uint32_t)X, (uint32_t)arow, (uint32_t)bsnp);
                     tk.offer(cd, thr, hi);
                 }
-                if (mode != kPairsStore) tk.check(hi, kCap - kEpiPerStep, bar);
+                if (!GCANDS && mode != kPairsStore) tk.check(hi, kCap - kEpiPerStep, bar);
             }
+            if constexpr (GCANDS) tk.check(hi, kCapG - kEpiPerTile, bar);
         }
         if (!ok) {
             record_error(P.err, 5);
@@ -1021,8 +1146,54 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
 
 }  // namespace tc
 
+// Largest distance |lngamma1_filter(v) - t32[v]| over kSmallTab <= v < size
+// (below kSmallTab the filter reads the table itself), as the bits of a
+// non-negative float rounded up (their integer order is the float order).
+__global__ void __launch_bounds__(256) k2_filter_error_kernel(const float* __restrict__ t32, int size,
+                                                               unsigned* __restrict__ out) {
+    float worst = 0.0f;
+    for (int v = kSmallTab + (int)(blockIdx.x * blockDim.x + threadIdx.x); v < size; v += (int)(gridDim.x * blockDim.x)) {
+        const double d = fabs((double)lngamma1_stirling(v) - (double)__ldg(t32 + v));
+        worst = fmaxf(worst, __double2float_ru(d));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) worst = fmaxf(worst, __shfl_xor_sync(0xFFFFFFFFu, worst, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(worst));
+}
+
 // ------------------------------------------------------------------ host
 using namespace tc;
+
+episdet_status k2_filter_margin(Workspace* w, int nc, int nn, const float* d_t32, float* margin) {
+    const int N = nc + nn, size = N + 2;
+    unsigned eps_bits = 0;
+    CUDA_TRY(w->flag.ensure(sizeof(int) * 4));
+    unsigned* d_out = (unsigned*)w->flag.p + 2;
+    CUDA_TRY(cudaMemsetAsync(d_out, 0, sizeof(unsigned), w->st));
+    if (size > kSmallTab) {
+        k2_filter_error_kernel<<<std::min((size + 255) / 256, 148 * 8), 256, 0, w->st>>>(d_t32, size, d_out);
+        CHECK_LAUNCH();
+    }
+    CUDA_TRY(cudaMemcpyAsync(&eps_bits, d_out, sizeof(unsigned), cudaMemcpyDeviceToHost, w->st));
+    CUDA_TRY(cudaStreamSynchronize(w->st));
+    float eps;
+    memcpy(&eps, &eps_bits, sizeof(eps));
+    // |S_fp32 - S_filter| <= 81 eps (81 table reads per 3-way table) + the
+    // rounding of both FP32 sums.  Rounding of one sum (27 cells, unit
+    // roundoff u = 2^-24): u * (sum_c |a_c| + |b_c| + |s_c|) with a_c the
+    // first addition of a cell, b_c the cell term, s_c the running sum; sum_c
+    // lnG(n_c + 1) <= lnG(n + 1) per class (superadditivity of ln n!), |b_c| <=
+    // (n_c + m_c) ln 2 + ln(N + 1) + 3 (b_c = -ln((n+m+1) C(n+m, n)) up to the
+    // table's error), |s_c| <= sum of the |b_c|.
+    const double u = std::ldexp(1.0, -24);
+    const double lg = std::lgamma((double)nc + 1.0) + std::lgamma((double)nn + 1.0) + 54.0;
+    const double bt = (double)N * std::log(2.0) + 27.0 * (std::log((double)N + 2.0) + 3.0);
+    const double round1 = u * (lg + 28.0 * bt) * 1.05;
+    const double m = 81.0 * (double)eps + 2.0 * round1 + 1.0;
+    *margin = std::nextafter((float)m, std::numeric_limits<float>::infinity());
+    w->d2h += (int64_t)sizeof(unsigned);
+    return EPISDET_OK;
+}
 
 static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 
@@ -1053,19 +1224,19 @@ static episdet_status make_tmap(CUtensorMap* m, void* base, uint64_t rows, uint6
 
 episdet_status tensor_init_attributes() {
     CUDA_TRY(cudaFuncSetAttribute(tc_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)Cfg<false>::kSmemTotal));
+                                  (int)KCfg<false, false>::kSmemTotal));
     CUDA_TRY(cudaFuncSetAttribute(tc_kernel<true, false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)Cfg<true>::kSmemTotal));
+                                  (int)KCfg<true, false, 0>::kSmemTotal));
     CUDA_TRY(cudaFuncSetAttribute(tc_kernel<true, true, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)Cfg<true, true>::kSmemTotal));
+                                  (int)KCfg<true, true, 0>::kSmemTotal));
     CUDA_TRY(cudaFuncSetAttribute(tc_kernel<true, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)Cfg<true>::kSmemTotal));
+                                  (int)KCfg<true, false, 1>::kSmemTotal));
     CUDA_TRY(cudaFuncSetAttribute(tc_kernel<true, true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)Cfg<true, true>::kSmemTotal));
+                                  (int)KCfg<true, true, 1>::kSmemTotal));
     CUDA_TRY(cudaFuncSetAttribute(tc_kernel<true, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)Cfg<true>::kSmemTotal));
+                                  (int)KCfg<true, false, 0, true>::kSmemTotal));
     CUDA_TRY(cudaFuncSetAttribute(tc_kernel<true, false, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)Cfg<true>::kSmemTotal));
+                                  (int)KCfg<true, false, 1, true>::kSmemTotal));
     return get_encoder();
 }
 
@@ -1143,7 +1314,7 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
         attr[0].val.clusterDim.z = 1;
         cfg.gridDim = dim3(2 * (grid / 2), 1, 1);
         cfg.blockDim = dim3(kThreads, 1, 1);
-        cfg.dynamicSmemBytes = Cfg<true>::kSmemTotal;
+        cfg.dynamicSmemBytes = mi ? KCfg<true, false, 1, true>::kSmemTotal : KCfg<true, false, 0, true>::kSmemTotal;
         cfg.stream = w->st;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
@@ -1220,7 +1391,7 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     p.mode = kPairsStore;
     p.pair_out0 = (uint4*)w->pair4[0].p;
     p.pair_out1 = (uint4*)w->pair4[1].p;
-    tc_kernel<false, false><<<std::max(1, std::min(grid, (int)ptiles.size())), kThreads, Cfg<false>::kSmemTotal, w->st>>>(tm2,
+    tc_kernel<false, false><<<std::max(1, std::min(grid, (int)ptiles.size())), kThreads, KCfg<false, false>::kSmemTotal, w->st>>>(tm2,
                                                                                                                p);
     CHECK_LAUNCH();
     ++*launches;
@@ -1258,13 +1429,16 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     }
     const int xend = std::min(fe, M - 2);
     p.mode = kTriplets;
+    CUDA_TRY(w->cbuf.ensure(sizeof(Cand) * (size_t)kCapG * grid));
+    p.cbuf = (Cand*)w->cbuf.p;
     // Large classes make the staged kernel's early release of segment 0 pay
     // (its MMAs then overlap the epilogue); smaller ones run the plain kernel.
     const bool staged = w->stage_override >= 0 ? w->stage_override == 1 : std::min(D.n[0], D.n[1]) >= kStageClass;
     // One instance per score, so each carries only its own scoring code.
     auto* const kern = staged ? (mi ? tc_kernel<true, true, 1> : tc_kernel<true, true, 0>)
                               : (mi ? tc_kernel<true, false, 1> : tc_kernel<true, false, 0>);
-    const size_t ksmem = staged ? Cfg<true, true>::kSmemTotal : Cfg<true>::kSmemTotal;
+    const size_t ksmem = mi ? (staged ? KCfg<true, true, 1>::kSmemTotal : KCfg<true, false, 1>::kSmemTotal)
+                            : (staged ? KCfg<true, true, 0>::kSmemTotal : KCfg<true, false, 0>::kSmemTotal);
     // CTA pairs: as many clusters of two as can be resident at once.
     int pairs = 0;
     {
