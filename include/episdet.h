@@ -80,6 +80,19 @@ enum { EPISDET_ENGINE_AUTO = 0, EPISDET_ENGINE_TENSOR = 1, EPISDET_ENGINE_SIMT =
  * memory and returns; the call then fails with EPISDET_ERR_TIMEOUT and the
  * device stays usable for the next call. */
 #define EPISDET_FLAG_INJECT_STALL 0x10u
+/* K2 triplet searches on the tensor engine bound each set's score without
+ * table reads and score exactly only the sets that can still enter the top-k
+ * list (same results either way).  By default this runs when every CTA scores
+ * far more sets than its candidate list holds (about 1.5e9 sets in the
+ * search); these flags force it on or off. */
+#define EPISDET_FLAG_FILTER_ON 0x20u
+#define EPISDET_FLAG_FILTER_OFF 0x40u
+/* episdet_search_perm with order 2 on the tensor engine counts, per label,
+ * only the cases' AND cells (the label as a third AND operand, by regrouping
+ * the case samples) and derives the controls' cells from the label-free
+ * pair counts, computed once per call.  This flag runs each label as a plain
+ * two-class search instead (same results). */
+#define EPISDET_FLAG_PERM_SPLIT 0x80u
 
 /* One cohort split into cases and controls (the reference's two .bin files). */
 typedef struct episdet_dataset {

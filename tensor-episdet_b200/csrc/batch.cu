@@ -13,6 +13,11 @@
 // A permutation is applied on the GPU: a label vector splits the cohort's
 // sample columns into case and control plane sets in the reference layout,
 // which then go through the ordinary search with device-resident inputs.
+// For 2-way searches on the tensor engine the label acts as a third AND
+// operand: the AND cells of every pair over all samples are counted once per
+// call, and per label only the cases' cells are counted (over the regrouped
+// case samples, half the MACs of counting both classes at a balanced split);
+// the controls' cells are the totals minus the cases'.
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -135,7 +140,8 @@ extern "C" episdet_status episdet_search_batched(const episdet_dataset* cohorts,
 // One label vector of a permutation batch: split the cohort's sample columns
 // into case and control plane sets on the GPU, then search them.
 static episdet_status perm_one(Workspace* w, const uint32_t* d_planes, int M, int n, int W, const uint32_t* label,
-                               bool label_on_device, const episdet_options& o, episdet_result* result) {
+                               bool label_on_device, bool first_label, const episdet_options& o,
+                               episdet_result* result) {
     std::vector<uint32_t> lab((size_t)W);
     std::vector<int> idx((size_t)n);
     if (!label_on_device)
@@ -174,7 +180,12 @@ static episdet_status perm_one(Workspace* w, const uint32_t* d_planes, int M, in
     d.num_controls = nn;
     d.memory = EPISDET_DEVICE;
     episdet_status st = check_dataset(&d, o.order);
-    if (st == EPISDET_OK) st = search_locked(w, &d, o, result);
+    // The planes of every label are columns of the cohort's, validated (when
+    // asked) with its first label; re-checking them per label would add a
+    // synchronising read-back each time.
+    episdet_options ol = o;
+    if (!first_label) ol.flags |= EPISDET_FLAG_NO_VALIDATE;
+    if (st == EPISDET_OK) st = search_locked(w, &d, ol, result);
     if (st == EPISDET_OK) result->kernel_launches += 2;
     return st;
 }
@@ -214,6 +225,18 @@ extern "C" episdet_status episdet_search_perm(const episdet_cohort* cohort, cons
         d_planes = (const uint32_t*)w0->perm_planes.p;
     }
     const bool on_device = cohort->memory == EPISDET_DEVICE;
+    // Label mode: the pair totals of the whole cohort, once, shared read-only
+    // by every lane (the computation ends with a synchronise of lane 0's stream).
+    const uint4* tot = nullptr;
+    const size_t tot_bytes = sizeof(uint4) * (size_t)M * (size_t)M;
+    if (o.order == 2 && o.engine != EPISDET_ENGINE_SIMT && !(o.flags & EPISDET_FLAG_PERM_SPLIT) &&
+        n <= kTensorMaxClass && tot_bytes <= (size_t)kLabelTotalsMaxBytes) {
+        begin_call(w0, o);
+        CUDA_TRY(w0->perm_tot.ensure(tot_bytes));
+        st = tensor_pair_totals(w0, d_planes, M, n, (uint4*)w0->perm_tot.p);
+        if (st != EPISDET_OK) return st;
+        tot = (const uint4*)w0->perm_tot.p;
+    }
     std::atomic<int32_t> next{0};
     std::atomic<bool> stop{false};
     std::mutex fail_mu;
@@ -237,7 +260,10 @@ extern "C" episdet_status episdet_search_perm(const episdet_cohort* cohort, cons
             if (p >= num_labels) return;
             clear_error();
             begin_call(w, o);
-            episdet_status s2 = perm_one(w, d_planes, M, n, W, labels + (size_t)p * W, on_device, o, &results[p]);
+            w->label_tot = tot;
+            episdet_status s2 =
+                perm_one(w, d_planes, M, n, W, labels + (size_t)p * W, on_device, p == 0, o, &results[p]);
+            w->label_tot = nullptr;
             if (s2 != EPISDET_OK) {
                 std::lock_guard<std::mutex> g(fail_mu);
                 if (fail_p < 0 || p < fail_p) fail_st = s2, fail_p = p, fail_msg = episdet_last_error();

@@ -53,6 +53,8 @@ struct Workspace {
     DevBuf xinfo;         // per-X segment tables (tensor engine)
     DevBuf tensor_flag;   // device error / progress words of the tensor engine
     DevBuf cbuf;          // per-CTA candidate buffers of the filtered triplet kernel
+    DevBuf perm_tot;      // label-free pair totals of a permutation batch's cohort
+    const uint4* label_tot = nullptr;  // set during a label-mode 2-way search (episdet_search_perm)
     DevBuf perm_planes, perm_cls[2], perm_idx;  // phenotype-permutation staging
     DevBuf bin_geno, bin_idx, bin_out[2];       // genotype-matrix binarizer staging
     // Per-call accounting.
@@ -71,7 +73,7 @@ struct Workspace {
         DevBuf* all[] = {&bits[0], &bits[1], &marg[0], &marg[1], &pair4[0], &pair4[1], &t32, &t64, &slots,
                          &counts, &tiles, &merged, &mcount, &fp64, &flag, &planes8, &xsub[0], &xsub[1], &xsub[2], &xsub[3], &xsub[4], &xsub[5],
                          &xsub[6], &xsub[7], &xinfo,
-                         &tensor_flag, &cbuf, &perm_planes, &perm_cls[0], &perm_cls[1], &perm_idx,
+                         &tensor_flag, &cbuf, &perm_tot, &perm_planes, &perm_cls[0], &perm_cls[1], &perm_idx,
                          &bin_geno, &bin_idx, &bin_out[0], &bin_out[1]};
         for (DevBuf* b : all) b->release();
         tab_score = tab_nc = tab_nn = -1;
@@ -91,6 +93,9 @@ episdet_status check_options(const episdet_options* in, int M, episdet_options* 
 episdet_status check_dataset(const episdet_dataset* d, int order);
 // Largest class the tensor engine counts exactly (FP32 accumulators: 2^24).
 constexpr int kTensorMaxClass = 1 << 24;
+// Largest label-free pair table (M x M x 16 bytes) a permutation batch builds
+// for its label mode; beyond it every label runs as a two-class search.
+constexpr long long kLabelTotalsMaxBytes = 32ll << 30;
 bool tensor_exact_for(const episdet_dataset* d);
 episdet_status check_engine(const episdet_dataset* d, const episdet_options& o);
 
@@ -108,6 +113,10 @@ episdet_status search_locked(Workspace* w, const episdet_dataset* data, const ep
 // Bound of the K2 scoring filter for a sample count (tensor.cu): measures the
 // filter's largest distance to the FP32 table d_t32 on the device.
 episdet_status k2_filter_margin(Workspace* w, int nc, int nn, const float* d_t32, float* margin);
+
+// Label-free AND cells of every pair of one plane set (tensor.cu), for the
+// label-mode 2-way permutation search.
+episdet_status tensor_pair_totals(Workspace* w, const uint32_t* d_planes, int M, int n, uint4* out);
 
 // Sets the tensor engine's kernel attributes on the current device.
 episdet_status tensor_init_attributes();

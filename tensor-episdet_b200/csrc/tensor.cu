@@ -143,6 +143,9 @@ struct TcParams {
     uint4* pair_out1;
     int* err;
     Cand* cbuf;        // kFeatGlobalCands instances: [grid][kCapG] candidate buffers in global memory
+    // 2-way label mode: [M][M] AND cells of every pair over all samples of the
+    // cohort; the controls' cells are these minus the cases' (no control MMAs).
+    const uint4* tot;
     uint64_t wait_ns;  // limit of every wait for work
     const int* hold;   // failure-detection test: a word the scoring warps wait for (nothing sets it), or null
 };
@@ -227,11 +230,19 @@ struct Cfg {
 // rows; operand prefetch (kFeatOpPrefetch) measured slower and is off.  The MI
 // triplet, 2-way and pair-table instances keep the plain layout (with MI's
 // exact scoring, larger stages cost the epilogue more L1 than they gained).
-template <bool PAIR, bool TWO, int SC>
-constexpr int kInstanceFeat =
-    (PAIR && !TWO && SC == 0) ? (kFeatFilter | kFeatBigStages | kFeatGlobalCands | kFeatPairPrefetch) : 0;
-template <bool PAIR, bool STAGE, int SC = -1, bool TWO = false>
-using KCfg = Cfg<PAIR, STAGE, kInstanceFeat<PAIR, TWO, SC>>;
+// VAR = 1 selects these features for a K2 triplet instance; the host runs it
+// for searches large enough that each CTA scores far more sets than its
+// candidate list holds (kFilterMinSetsPerCta), and the plain K2 instance
+// (VAR = 0, exact scoring from a shared-memory table) for smaller ones, where
+// the filter's warm-up -- every set scored exactly until the lists fill --
+// is most of the search.
+template <bool PAIR, bool TWO, int SC, int VAR>
+constexpr int kInstanceFeat = (PAIR && !TWO && SC == 0 && VAR == 1)
+                                  ? (kFeatFilter | kFeatBigStages | kFeatGlobalCands | kFeatPairPrefetch)
+                                  : 0;
+template <bool PAIR, bool STAGE, int SC = -1, bool TWO = false, int VAR = 0>
+using KCfg = Cfg<PAIR, STAGE, kInstanceFeat<PAIR, TWO, SC, VAR>>;
+constexpr double kFilterMinSetsPerCta = 1.0e7;
 
 // Per-launch copy of each group member's segments in shared memory.
 struct GroupSm {
@@ -577,16 +588,16 @@ __device__ __forceinline__ void record_error(int* err, int code) { atomicCAS(err
 // without table reads (k2_approx32); only sets that may be better than the
 // CTA's current k-th candidate are scored exactly (from the global table),
 // so the candidate lists are those of scoring every set.
-template <bool PAIR, bool STAGE, int SC = -1, bool TWO = false>
+template <bool PAIR, bool STAGE, int SC = -1, bool TWO = false, int VAR = 0>
 __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
     tc_kernel(const __grid_constant__ TmapPack tm, const __grid_constant__ TcParams P) {
     static_assert(PAIR || !STAGE, "staging is a pair-kernel mode");
     static_assert(!TWO || (PAIR && !STAGE), "the 2-way pair kernel is the plain pair instance");
-    using C = KCfg<PAIR, STAGE, SC, TWO>;
+    using C = KCfg<PAIR, STAGE, SC, TWO, VAR>;
     constexpr bool FILTER = C::FILTER;
     constexpr bool GCANDS = C::GCANDS;
-    constexpr bool OPF = (kInstanceFeat<PAIR, TWO, SC> & kFeatOpPrefetch) != 0;
-    constexpr bool PPF = (kInstanceFeat<PAIR, TWO, SC> & kFeatPairPrefetch) != 0;
+    constexpr bool OPF = (kInstanceFeat<PAIR, TWO, SC, VAR> & kFeatOpPrefetch) != 0;
+    constexpr bool PPF = (kInstanceFeat<PAIR, TWO, SC, VAR> & kFeatPairPrefetch) != 0;
     constexpr int kStages = C::kStages;
     constexpr int kStageBytes = C::kStageBytes;
     constexpr int kKbBytes = C::kKbBytes;
@@ -963,7 +974,8 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
             int xy9[2][9];
             const int X = s_grp[g].x;
             const bool row_ok = arow < M && (mode != kTriplets || arow > X);
-            if (row_ok) {
+            // (store mode needs no marginals: the pair-total launch passes none)
+            if (row_ok && mode != kPairsStore) {
 #pragma unroll
                 for (int c = 0; c < 2; ++c) load_marg3(P.D.marg[c], M, arow, ma[c]);
                 if (mode == kTriplets) {
@@ -1041,7 +1053,8 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                         if (row_ok && arow < bsnp && bsnp < M) {
                             size_t o = (size_t)arow * M + bsnp;
                             P.pair_out0[o] = make_uint4(cnt(0, 0, 0), cnt(0, 0, 1), cnt(0, 1, 0), cnt(0, 1, 1));
-                            P.pair_out1[o] = make_uint4(cnt(1, 0, 0), cnt(1, 0, 1), cnt(1, 1, 0), cnt(1, 1, 1));
+                            if (P.pair_out1)
+                                P.pair_out1[o] = make_uint4(cnt(1, 0, 0), cnt(1, 0, 1), cnt(1, 1, 0), cnt(1, 1, 1));
                         }
                         continue;
                     }
@@ -1055,10 +1068,19 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                         cs[4] = cnt(0, 1, 1);
                         load_marg3(P.D.marg[0], M, bsnp, mb);
                         derive9(cs, ma[0], mb);
-                        cn[0] = cnt(1, 0, 0);
-                        cn[1] = cnt(1, 0, 1);
-                        cn[3] = cnt(1, 1, 0);
-                        cn[4] = cnt(1, 1, 1);
+                        if (P.tot) {
+                            // Label mode: controls = all samples - cases.
+                            const uint4 t = __ldg(P.tot + (size_t)arow * M + bsnp);
+                            cn[0] = (int)t.x - cs[0];
+                            cn[1] = (int)t.y - cs[1];
+                            cn[3] = (int)t.z - cs[3];
+                            cn[4] = (int)t.w - cs[4];
+                        } else {
+                            cn[0] = cnt(1, 0, 0);
+                            cn[1] = cnt(1, 0, 1);
+                            cn[3] = cnt(1, 1, 0);
+                            cn[4] = cnt(1, 1, 1);
+                        }
                         load_marg3(P.D.marg[1], M, bsnp, mb);
                         derive9(cn, ma[1], mb);
                         float sc = score32_lut<9, LutShared, SC>(P.T, lut, cs, cn);
@@ -1222,6 +1244,66 @@ static episdet_status make_tmap(CUtensorMap* m, void* base, uint64_t rows, uint6
     return EPISDET_OK;
 }
 
+static int grid_for(long work, int threads) {
+    long b = (work + threads - 1) / threads;
+    return (int)std::min<long>(std::max<long>(b, 1), 148L * 64);
+}
+
+// Label-free AND cells of every SNP pair over the n samples of one plane set
+// ([M][2][W] words, on the device) into out ([M][M] uint4, pairs a < b): the
+// pair-table kernel over a single class.
+episdet_status tensor_pair_totals(Workspace* w, const uint32_t* d_planes, int M, int n, uint4* out) {
+    episdet_status st = get_encoder();
+    if (st != EPISDET_OK) return st;
+    CUDA_TRY(w->tensor_flag.ensure(sizeof(int) * 4));
+    CUDA_TRY(cudaMemsetAsync(w->tensor_flag.p, 0, sizeof(int) * 4, w->st));
+    DevData D;
+    memset(&D, 0, sizeof(D));
+    D.M = M;
+    D.bits[0] = d_planes;
+    D.bits[1] = d_planes;  // no second class: W[1] = 0
+    D.n[0] = n;
+    D.W[0] = episdet_class_words(n);
+    const int Kc = D.W[0] * 32, rows = 2 * M, pitch2 = Kc;
+    CUDA_TRY(w->planes8.ensure((size_t)rows * pitch2));
+    uint8_t* P2 = (uint8_t*)w->planes8.p;
+    unpack_kernel<<<grid_for((long)rows * (pitch2 / 16), 256), 256, 0, w->st>>>(D, P2, rows, pitch2);
+    CHECK_LAUNCH();
+    TmapPack tm2;
+    memset(&tm2, 0, sizeof(tm2));
+    st = make_tmap(&tm2.m[0], P2, (uint64_t)rows, (uint64_t)pitch2);
+    if (st != EPISDET_OK) return st;
+    const int nt = (M + kTileSnps - 1) / kTileSnps;
+    std::vector<int2> ptiles;
+    for (int a = 0; a < nt; ++a)
+        for (int b = a; b < nt; ++b) ptiles.push_back(make_int2(a, b));
+    CUDA_TRY(w->tiles.ensure(sizeof(int2) * ptiles.size()));
+    CUDA_TRY(cudaMemcpyAsync(w->tiles.p, ptiles.data(), sizeof(int2) * ptiles.size(), cudaMemcpyHostToDevice, w->st));
+    TcParams p;
+    memset(&p, 0, sizeof(p));
+    p.D = D;
+    p.first_begin = 0;
+    p.first_end = M;
+    p.err = (int*)w->tensor_flag.p;
+    p.wait_ns = 4000ull * 1000000ull;
+    p.ngroup = 1;
+    p.grp[0] = GroupDesc{(const int2*)w->tiles.p, 0, -1, nullptr};
+    p.ntiles = (int)ptiles.size();
+    p.mode = kPairsStore;
+    p.seg2[0] = Seg{0, Kc / kKB};
+    p.seg2[1] = Seg{Kc / kKB, Kc / kKB};
+    p.pair_out0 = out;
+    p.pair_out1 = nullptr;
+    tc_kernel<false, false><<<std::max(1, std::min(w->sms, (int)ptiles.size())), kThreads,
+                              KCfg<false, false>::kSmemTotal, w->st>>>(tm2, p);
+    CHECK_LAUNCH();
+    int err = 0;
+    CUDA_TRY(cudaMemcpyAsync(&err, w->tensor_flag.p, sizeof(int), cudaMemcpyDeviceToHost, w->st));
+    CUDA_TRY(cudaStreamSynchronize(w->st));  // the tile list is reused by the next search
+    if (err) return set_error(EPISDET_ERR_TIMEOUT, "a bounded device wait gave up (code %d)", err);
+    return EPISDET_OK;
+}
+
 episdet_status tensor_init_attributes() {
     CUDA_TRY(cudaFuncSetAttribute(tc_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)KCfg<false, false>::kSmemTotal));
@@ -1229,6 +1311,10 @@ episdet_status tensor_init_attributes() {
                                   (int)KCfg<true, false, 0>::kSmemTotal));
     CUDA_TRY(cudaFuncSetAttribute(tc_kernel<true, true, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)KCfg<true, true, 0>::kSmemTotal));
+    CUDA_TRY(cudaFuncSetAttribute(tc_kernel<true, false, 0, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)KCfg<true, false, 0, false, 1>::kSmemTotal));
+    CUDA_TRY(cudaFuncSetAttribute(tc_kernel<true, true, 0, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)KCfg<true, true, 0, false, 1>::kSmemTotal));
     CUDA_TRY(cudaFuncSetAttribute(tc_kernel<true, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)KCfg<true, false, 1>::kSmemTotal));
     CUDA_TRY(cudaFuncSetAttribute(tc_kernel<true, true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1240,10 +1326,6 @@ episdet_status tensor_init_attributes() {
     return get_encoder();
 }
 
-static int grid_for(long work, int threads) {
-    long b = (work + threads - 1) / threads;
-    return (int)std::min<long>(std::max<long>(b, 1), 148L * 64);
-}
 
 episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const episdet_options& o, int fb, int fe,
                           Slots* S, uint64_t* launches, bool progress) {
@@ -1278,10 +1360,15 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
         // Pairs on the CTA-pair kind::mxf4 kernel: packed e2m1 rows of every
         // SNP plane, tiles of 128 A SNPs x 56 B SNPs whose B range reaches
         // past the tile's first A SNP, two accumulator sets in TMEM.
-        const int pitchx = (Kc + kClassPad) / 2 + (Kn + kClassPad) / 2;
+        // Label mode (w->label_tot): operand rows of the cases only; the
+        // controls' cells come from the label-free pair totals.
+        const bool label = w->label_tot != nullptr;
+        const int pitchx = (Kc + kClassPad) / 2 + (label ? 0 : (Kn + kClassPad) / 2);
         CUDA_TRY(w->xsub[0].ensure((size_t)rows * pitchx));
         uint8_t* F = (uint8_t*)w->xsub[0].p;
-        pack_f4_kernel<<<grid_for((long)rows * (D.W[0] + D.W[1]), 256), 256, 0, w->st>>>(D, F, rows, pitchx);
+        DevData Dp = D;
+        if (label) Dp.W[1] = 0;  // pack class 0 only
+        pack_f4_kernel<<<grid_for((long)rows * (Dp.W[0] + Dp.W[1]), 256), 256, 0, w->st>>>(Dp, F, rows, pitchx);
         CHECK_LAUNCH();
         ++*launches;
         TmapPack tmf;
@@ -1300,7 +1387,8 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
         w->h2d += (int64_t)(sizeof(int2) * tiles.size());
         const int kb1 = (Kc + kClassPad) / kF4PerKB;
         p.seg2[0] = Seg{0, (D.n[0] + kF4PerKB - 1) / kF4PerKB};
-        p.seg2[1] = Seg{kb1, kb1 + (D.n[1] + kF4PerKB - 1) / kF4PerKB};
+        p.seg2[1] = label ? Seg{kb1, kb1} : Seg{kb1, kb1 + (D.n[1] + kF4PerKB - 1) / kF4PerKB};
+        p.tot = w->label_tot;
         p.ngroup = 1;
         p.grp[0] = GroupDesc{(const int2*)w->tiles.p, 0, -1, nullptr};
         p.ntiles = (int)tiles.size();
@@ -1435,10 +1523,19 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     // (its MMAs then overlap the epilogue); smaller ones run the plain kernel.
     const bool staged = w->stage_override >= 0 ? w->stage_override == 1 : std::min(D.n[0], D.n[1]) >= kStageClass;
     // One instance per score, so each carries only its own scoring code.
-    auto* const kern = staged ? (mi ? tc_kernel<true, true, 1> : tc_kernel<true, true, 0>)
-                              : (mi ? tc_kernel<true, false, 1> : tc_kernel<true, false, 0>);
+    // K2: the filtered instance for searches where every CTA scores far more
+    // sets than its candidate list holds (or as the flags force).
+    double slab_sets = 0.0;
+    for (int x = fb; x < xend; ++x) slab_sets += 0.5 * (double)(M - 1 - x) * (double)(M - 2 - x);
+    const bool filt = !mi && (o.flags & EPISDET_FLAG_FILTER_OFF) == 0 &&
+                      ((o.flags & EPISDET_FLAG_FILTER_ON) != 0 || slab_sets >= kFilterMinSetsPerCta * (double)grid);
+    auto* const kern = mi ? (staged ? tc_kernel<true, true, 1> : tc_kernel<true, false, 1>)
+                          : filt ? (staged ? tc_kernel<true, true, 0, false, 1> : tc_kernel<true, false, 0, false, 1>)
+                                 : (staged ? tc_kernel<true, true, 0> : tc_kernel<true, false, 0>);
     const size_t ksmem = mi ? (staged ? KCfg<true, true, 1>::kSmemTotal : KCfg<true, false, 1>::kSmemTotal)
-                            : (staged ? KCfg<true, true, 0>::kSmemTotal : KCfg<true, false, 0>::kSmemTotal);
+                            : filt ? (staged ? KCfg<true, true, 0, false, 1>::kSmemTotal
+                                             : KCfg<true, false, 0, false, 1>::kSmemTotal)
+                                   : (staged ? KCfg<true, true, 0>::kSmemTotal : KCfg<true, false, 0>::kSmemTotal);
     // CTA pairs: as many clusters of two as can be resident at once.
     int pairs = 0;
     {

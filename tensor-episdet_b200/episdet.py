@@ -25,6 +25,8 @@ ENGINE_AUTO, ENGINE_TENSOR, ENGINE_SIMT = 0, 1, 2
 FLAG_PROGRESS, FLAG_NO_VALIDATE, FLAG_TIMING = 0x1, 0x2, 0x4
 FLAG_AUTOTUNE = 0x8  # measure the triplet instance per shape and cache the choice
 FLAG_INJECT_STALL = 0x10  # testing aid: every tensor launch waits on a word nothing sets and times out
+FLAG_FILTER_ON, FLAG_FILTER_OFF = 0x20, 0x40  # force the K2 triplet scoring filter on / off
+FLAG_PERM_SPLIT = 0x80  # permutation search: a plain two-class search per label instead of label mode
 
 STATUS = {
     0: "EPISDET_OK",
@@ -440,14 +442,14 @@ def search_batched(cohorts, options) -> list:
 
 
 def search_perm(planes, num_samples: int, labels, *, order: int = 2, score="k2", top_k: int = 1024, device: int = 0,
-                engine="auto") -> list:
+                engine="auto", flags: int = 0) -> list:
     pp, mp = _ptr(planes)
     pl, ml = _ptr(labels)
     if mp != ml:
         raise TypeError("planes and labels must live in the same memory")
     nl = int(labels.shape[0])
     c = Cohort(pp, int(planes.shape[0]), num_samples, mp)
-    o = make_options(order, score, top_k, device, engine)
+    o = make_options(order, score, top_k, device, engine, flags=flags)
     rs = (Result * nl)()
     keep = []
     for i in range(nl):

@@ -27,11 +27,13 @@ def perm(a):
     planes = episdet.generate_cohort(a.seed, a.snps, n, maf=tuple(a.maf))
     labels = episdet.generate_labels(a.seed + 1, n, a.cases, a.permutations)
     t0 = time.perf_counter()
-    res = episdet.search_perm(planes, n, labels, order=a.order, score=a.score, top_k=a.top_k)
+    res = episdet.search_perm(planes, n, labels, order=a.order, score=a.score, top_k=a.top_k, flags=a.flags)
     dt = time.perf_counter() - t0
     best = np.array([r.score for r in res])
     sets = sum(r.sets_evaluated for r in res)
     print(json.dumps({"permutations": len(res), "seconds": dt, "device_ms": sum(r.device_ms for r in res),
+                      "count_kernel_ms": sum(r.count_kernel_ms for r in res),
+                      "executed_macs": sum(r.executed_macs for r in res),
                       "sets": sets, "tera_sets_samples_per_s": sets * n / dt / 1e12,
                       "label0_best": [list(res[0].snps), res[0].score],
                       "null_best_scores": {"min": float(best[1:].min()), "median": float(np.median(best[1:])),
@@ -59,6 +61,8 @@ def main():
                     help="planted sets, comma-separated SNP indices, sets separated by ';' (e.g. 137,2048,3901)")
     ap.add_argument("--base-risk", type=float, default=0.5)
     ap.add_argument("--effect", type=float, default=0.25)
+    ap.add_argument("--flags", type=lambda v: int(v, 0), default=0,
+                    help="extra EPISDET_FLAG_* bits (e.g. 0x20 forces the K2 triplet scoring filter on)")
     ap.add_argument("--permutations", type=int, default=0,
                     help="search one cohort of cases+controls samples under this many label vectors "
                          "(label 0 the first half of the samples, the rest seeded permutations)")
@@ -72,7 +76,7 @@ def main():
     for i in range(a.repeat):
         r = episdet.search(cases, controls, a.cases, a.controls, order=a.order, score=a.score, top_k=a.top_k,
                            engine=a.engine, first_begin=a.first_begin, first_end=a.first_end,
-                           flags=episdet.FLAG_TIMING)
+                           flags=episdet.FLAG_TIMING | a.flags)
     n = a.cases + a.controls
     out = {"snps": list(r.snps), "score": r.score, "sets": r.sets_evaluated, "device_ms": r.device_ms,
            "count_kernel_ms": r.count_kernel_ms, "count_launches": r.count_kernel_launches,

@@ -54,6 +54,11 @@ def test_random_datasets(episdet, oracle, order, M, nc, nn, score, engine):
     o = oracle.search(cases, controls, nc, nn, order=order, score=score, top_k=k)
     assert_same(r, o, k)
     assert r.sets_evaluated == o["sets"]
+    if order == 3 and score == "k2" and engine == "tensor":
+        # The kernel with the K2 scoring filter, forced on at this small size.
+        r = episdet.search(cases, controls, nc, nn, order=3, score="k2", top_k=k, engine="tensor",
+                           flags=episdet.FLAG_FILTER_ON)
+        assert_same(r, o, k)
 
 
 @pytest.mark.parametrize("engine", ENGINES)
@@ -73,10 +78,12 @@ def test_large_classes_triplets(episdet, oracle, score):
     meet in one launch."""
     cases, controls = episdet.generate(0xE91A, 44, 70000, 66000, maf=(0.02, 0.5))
     k = 256
-    r = episdet.search(cases, controls, 70000, 66000, order=3, score=score, top_k=k, engine="tensor")
     o = oracle.search(cases, controls, 70000, 66000, order=3, score=score, top_k=k)
-    assert_same(r, o, k)
-    assert r.sets_evaluated == o["sets"]
+    for flags in ((episdet.FLAG_FILTER_OFF, episdet.FLAG_FILTER_ON) if score == "k2" else (0,)):
+        r = episdet.search(cases, controls, 70000, 66000, order=3, score=score, top_k=k, engine="tensor",
+                           flags=flags)
+        assert_same(r, o, k)
+        assert r.sets_evaluated == o["sets"]
 
 
 @pytest.mark.parametrize("engine", ENGINES)
@@ -142,15 +149,23 @@ def test_invalid_planes_rejected(episdet):
     assert len(r.snps) == 2
 
 
-def test_permutations_match_split_searches(episdet, oracle):
-    n, M = 3000, 80
-    planes = episdet.generate_cohort(21, M, n)
-    labels = episdet.generate_labels(22, n, 1400, 4)
-    res = episdet.search_perm(planes, n, labels, order=2, score="k2", top_k=64)
-    for lab, r in zip(labels, res):
+@pytest.mark.parametrize("score", ["k2", "mi"])
+@pytest.mark.parametrize("n,M,ncase,nl", [(3000, 80, 1400, 4), (20011, 300, 6100, 5)])
+def test_permutations_match_split_searches(episdet, oracle, n, M, ncase, nl, score):
+    """Label mode (the label as a third AND operand: only the cases' cells are
+    counted per label, the controls' derived from the label-free totals), a
+    plain two-class search per label, and the integer-pipe engine, each against
+    the oracle on the split of every label."""
+    planes = episdet.generate_cohort(21 + n, M, n)
+    labels = episdet.generate_labels(22 + n, n, ncase, nl)
+    want = []
+    for lab in labels:
         cases, controls, nc, nn = oracle.split_by_label(planes, n, lab)
-        o = oracle.search(cases, controls, nc, nn, order=2, score="k2", top_k=64)
-        assert_same(r, o, 64)
+        want.append(oracle.search(cases, controls, nc, nn, order=2, score=score, top_k=64))
+    for engine, flags in (("auto", 0), ("auto", episdet.FLAG_PERM_SPLIT), ("simt", 0)):
+        res = episdet.search_perm(planes, n, labels, order=2, score=score, top_k=64, engine=engine, flags=flags)
+        for r, o in zip(res, want):
+            assert_same(r, o, 64)
 
 
 def test_perm_pvalues_of_a_permutation_search(episdet):

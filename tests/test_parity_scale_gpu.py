@@ -40,12 +40,15 @@ def test_bench_workload_slabs(episdet, oracle, cfg2, slab):
     cases, controls = cfg2
     fb, fe = slab
     k = 1024
-    r = episdet.search(cases, controls, CFG2["nc"], CFG2["nn"], order=3, score="k2", top_k=k, engine="tensor",
-                       first_begin=fb, first_end=fe)
     o = oracle.search(cases, controls, CFG2["nc"], CFG2["nn"], order=3, score="k2", top_k=k, first_begin=fb,
                       first_end=fe)
-    assert_same(r, o, k)
-    assert r.sets_evaluated == o["sets"]
+    # Both K2 triplet kernels: exact scoring, and the scoring filter (which a
+    # full search of this size runs).
+    for flags in (episdet.FLAG_FILTER_OFF, episdet.FLAG_FILTER_ON):
+        r = episdet.search(cases, controls, CFG2["nc"], CFG2["nn"], order=3, score="k2", top_k=k, engine="tensor",
+                           first_begin=fb, first_end=fe, flags=flags)
+        assert_same(r, o, k)
+        assert r.sets_evaluated == o["sets"]
 
 
 def test_mi_workload_slab(episdet, oracle):
@@ -67,11 +70,12 @@ def test_tile_list_and_band_edges(episdet, oracle, score):
     M, nc, nn = 1024, 10000, 10000
     cases, controls = episdet.generate(0x5CA1E, M, nc, nn)
     k = 1024
-    r = episdet.search(cases, controls, nc, nn, order=3, score=score, top_k=k, engine="tensor", first_begin=250,
-                       first_end=260)
     o = oracle.search(cases, controls, nc, nn, order=3, score=score, top_k=k, first_begin=250, first_end=260)
-    assert_same(r, o, k)
-    assert r.sets_evaluated == o["sets"]
+    for flags in ((episdet.FLAG_FILTER_OFF, episdet.FLAG_FILTER_ON) if score == "k2" else (0,)):
+        r = episdet.search(cases, controls, nc, nn, order=3, score=score, top_k=k, engine="tensor",
+                           first_begin=250, first_end=260, flags=flags)
+        assert_same(r, o, k)
+        assert r.sets_evaluated == o["sets"]
 
 
 def test_class_past_fp32_exactness_goes_to_the_integer_engine(episdet, oracle):
