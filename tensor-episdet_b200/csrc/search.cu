@@ -99,7 +99,7 @@ episdet_status get_workspace_lane(int device, int lane, Workspace** out) {
         CUDA_TRY(cudaStreamCreateWithFlags(&w->own_st, cudaStreamNonBlocking));
         CUDA_TRY(cudaStreamCreateWithFlags(&w->aux_st, cudaStreamNonBlocking));
         CUDA_TRY(cudaEventCreateWithFlags(&w->ev_ready, cudaEventDisableTiming));
-        for (int i = 0; i < 2; ++i) {
+        for (int i = 0; i < kXSets; ++i) {
             CUDA_TRY(cudaEventCreateWithFlags(&w->ev_cmp[i], cudaEventDisableTiming));
             CUDA_TRY(cudaEventCreateWithFlags(&w->ev_tc[i], cudaEventDisableTiming));
         }

@@ -38,18 +38,23 @@ struct DevBuf {
     void release();
 };
 
+// Sets of regrouped operand buffers of the triplet engine: the regrouping of
+// group g + kXSets - 1 (second stream) overlaps the counting launch of group g.
+constexpr int kXSets = 2;
+constexpr int kXGroup = 4;  // first SNPs per triplet launch (tc::kMaxGroup)
+
 struct Workspace {
     int device = 0;
     int sms = 0;
     cudaStream_t st = nullptr;      // stream of the current call (own_st or the caller's)
     cudaStream_t own_st = nullptr;  // the library's own stream
     cudaStream_t aux_st = nullptr;  // operand regrouping, overlapped with the counting launches
-    cudaEvent_t ev_ready = nullptr, ev_cmp[2] = {}, ev_tc[2] = {};  // ordering between st and aux_st
+    cudaEvent_t ev_ready = nullptr, ev_cmp[kXSets] = {}, ev_tc[kXSets] = {};  // ordering between st and aux_st
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     std::mutex mu;
     DevBuf bits[2], marg[2], pair4[2], t32, t64, slots, counts, tiles, merged, mcount, fp64, flag;
     DevBuf planes8;       // unpacked 0/1 byte operand rows (tensor engine)
-    DevBuf xsub[8];       // per-X sample-regrouped operand rows (tensor engine)
+    DevBuf xsub[kXSets * kXGroup];  // per-X sample-regrouped operand rows (tensor engine)
     DevBuf xinfo;         // per-X segment tables (tensor engine)
     DevBuf tensor_flag;   // device error / progress words of the tensor engine
     DevBuf cbuf;          // per-CTA candidate buffers of the filtered triplet kernel
@@ -70,9 +75,9 @@ struct Workspace {
     double inv64 = 0.0, hy64 = 0.0;
 
     void release_all() {
+        for (DevBuf& b : xsub) b.release();
         DevBuf* all[] = {&bits[0], &bits[1], &marg[0], &marg[1], &pair4[0], &pair4[1], &t32, &t64, &slots,
-                         &counts, &tiles, &merged, &mcount, &fp64, &flag, &planes8, &xsub[0], &xsub[1], &xsub[2], &xsub[3], &xsub[4], &xsub[5],
-                         &xsub[6], &xsub[7], &xinfo,
+                         &counts, &tiles, &merged, &mcount, &fp64, &flag, &planes8, &xinfo,
                          &tensor_flag, &cbuf, &perm_tot, &perm_planes, &perm_cls[0], &perm_cls[1], &perm_idx,
                          &bin_geno, &bin_idx, &bin_out[0], &bin_out[1]};
         for (DevBuf* b : all) b->release();

@@ -109,7 +109,7 @@ struct XInfo {
     Seg seg[4];     // [class*2 + kept genotype]
 };
 
-constexpr int kMaxGroup = 4;  // first SNPs (X) per triplet launch
+constexpr int kMaxGroup = kXGroup;  // first SNPs (X) per triplet launch
 constexpr int kStageMin = kStageMinSamples;  // samples of segment 0 from which the staged kernel copies it out
 constexpr int kStageClass = 32768;  // class size from which triplet launches use the staged kernel
 constexpr int kBand = 12;     // tile-band edge of the triplet tile order
@@ -1488,17 +1488,17 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     // Regrouped rows: both classes' packed e2m1 regions, 2 samples per byte.
     const int pitchx = (Kc + kClassPad) / 2 + (Kn + kClassPad) / 2;
     const int max_n = std::max(D.n[0], D.n[1]);
-    for (int i = 0; i < 2 * kMaxGroup; ++i) CUDA_TRY(w->xsub[i].ensure((size_t)rows * pitchx));
-    // Two sets of regrouped operands and segment tables: the regrouping of
-    // group g + 1 (on aux_st) overlaps the counting launch of group g (on st).
+    for (int i = 0; i < kXSets * kMaxGroup; ++i) CUDA_TRY(w->xsub[i].ensure((size_t)rows * pitchx));
+    // kXSets sets of regrouped operands and segment tables: the regrouping of
+    // the next groups (on aux_st) overlaps the counting launch of group g (on st).
     const size_t info_bytes = 256;
     const size_t idx_bytes = sizeof(int) * 4 * (size_t)max_n;
-    CUDA_TRY(w->xinfo.ensure(2 * kMaxGroup * (info_bytes + idx_bytes)));
-    TmapPack tmx[2];
-    XInfo* d_info[2][kMaxGroup];
-    XWork xw[2];
-    CmpOut co[2];
-    for (int b = 0; b < 2; ++b) {
+    CUDA_TRY(w->xinfo.ensure(kXSets * kMaxGroup * (info_bytes + idx_bytes)));
+    TmapPack tmx[kXSets];
+    XInfo* d_info[kXSets][kMaxGroup];
+    XWork xw[kXSets];
+    CmpOut co[kXSets];
+    for (int b = 0; b < kXSets; ++b) {
         memset(&tmx[b], 0, sizeof(tmx[b]));
         xw[b].base = (uint8_t*)w->xinfo.p + (size_t)b * kMaxGroup * (info_bytes + idx_bytes);
         xw[b].stride = info_bytes + idx_bytes;
@@ -1561,10 +1561,10 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     int gi = 0;
     for (int x0 = fb; x0 < xend; x0 += kMaxGroup, ++gi) {
         const int gn = std::min(kMaxGroup, xend - x0);
-        const int b = gi & 1;
+        const int b = gi % kXSets;
         // Index lists and regrouped rows of the gn first SNPs, one launch each,
         // into buffer set b once the counting launch that last read it is done.
-        if (gi >= 2) CUDA_TRY(cudaStreamWaitEvent(w->aux_st, w->ev_tc[b], 0));
+        if (gi >= kXSets) CUDA_TRY(cudaStreamWaitEvent(w->aux_st, w->ev_tc[b], 0));
         xw[b].x0 = x0;
         xinfo_kernel<<<dim3(2, gn), kXinfoThreads, 0, w->aux_st>>>(D, xw[b]);
         CHECK_LAUNCH();
