@@ -234,11 +234,18 @@ int od_tables_build(int32_t score, int32_t num_cases, int32_t num_controls, od_t
             t->t32[v] = (float)log2((double)v * (double)t->inv_n32);
             t->t64[v] = log2((double)v / (double)N);
         }
-        /* H(Y), scoring.hpp:29-30, evaluated once in double. */
+        /* H(Y), scoring.hpp:29-30.  FP64 score: in double throughout.  FP32
+         * score: as the reference's device code evaluates those two lines --
+         * p = n * invN as a float product, the first term a double product
+         * rounded to float, the second a double fused multiply-add (nvcc
+         * contracts `entropyY += (-1.0) * p * t`) rounded to float. */
         double p1 = (double)num_cases * t->inv_n64;
         double p2 = (double)num_controls * t->inv_n64;
         t->hy64 = -(p1 * t->t64[num_cases]) - (p2 * t->t64[num_controls]);
-        t->hy32 = (float)t->hy64;
+        float q1 = (float)num_cases * t->inv_n32;
+        float hy = (float)(-((double)q1 * (double)t->t32[num_cases]));
+        float q2 = (float)num_controls * t->inv_n32;
+        t->hy32 = (float)fma(-(double)q2, (double)t->t32[num_controls], (double)hy);
     }
     return 0;
 }

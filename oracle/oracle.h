@@ -46,7 +46,7 @@ typedef struct od_tables {
     double* t64;
     float inv_n32;        /* MI: (float)(1.0/N) */
     double inv_n64;       /* MI: 1.0/N */
-    float hy32;           /* MI: class entropy H(Y), rounded to float */
+    float hy32;           /* MI: class entropy H(Y) in the FP32 score's own evaluation order */
     double hy64;
 } od_tables;
 

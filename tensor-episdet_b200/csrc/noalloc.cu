@@ -201,7 +201,7 @@ static episdet_status search_locked(const episdet_dataset* data, const episdet_o
         }
         double p1 = (double)nc * T.inv_n64, p2 = (double)nn * T.inv_n64;
         T.hy64 = -(p1 * h_t64[nc]) - (p2 * h_t64[nn]);
-        T.hy32 = (float)T.hy64;
+        T.hy32 = mi_hy32(nc, nn, T.inv_n32, h_t32);
     }
     T.score = o.score;
     T.t32 = (const float*)(S + kOffT32);

@@ -173,7 +173,7 @@ episdet_status build_tables(Workspace* w, int score, int nc, int nn, ScoreTables
             }
             double p1 = (double)nc * w->inv64, p2 = (double)nn * w->inv64;
             w->hy64 = -(p1 * t64[nc]) - (p2 * t64[nn]);
-            w->hy32 = (float)w->hy64;
+            w->hy32 = mi_hy32(nc, nn, w->inv32, t32.data());
         }
         CUDA_TRY(w->t32.ensure(sizeof(float) * size));
         CUDA_TRY(w->t64.ensure(sizeof(double) * size));

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstddef>
 #include <cstdint>
 #include <mutex>
@@ -101,6 +102,18 @@ constexpr int kTensorMaxClass = 1 << 24;
 // Largest label-free pair table (M x M x 16 bytes) a permutation batch builds
 // for its label mode; beyond it every label runs as a two-class search.
 constexpr long long kLabelTotalsMaxBytes = 32ll << 30;
+// H(Y) of the FP32 MI score as include/scoring.hpp:29-30 evaluates it on the
+// device: each class's p = n * (1/N) is a float product; the first term is a
+// double product rounded to float, the second a double multiply-add (nvcc
+// contracts `entropyY += (-1.0) * p * t` into one fused operation) rounded to
+// float.  t32 is the FP32 log2 table, indexed by count.
+inline float mi_hy32(int nc, int nn, float inv32, const float* t32) {
+    float p1 = (float)nc * inv32;
+    float hy = (float)(-((double)p1 * (double)t32[nc]));
+    float p2 = (float)nn * inv32;
+    return (float)std::fma(-(double)p2, (double)t32[nn], (double)hy);
+}
+
 bool tensor_exact_for(const episdet_dataset* d);
 episdet_status check_engine(const episdet_dataset* d, const episdet_options& o);
 
