@@ -126,7 +126,15 @@ typedef struct episdet_options {
      * copy, an MMA commit, the scoring warps) may take before the launch gives
      * up and the call returns EPISDET_ERR_TIMEOUT; 0 = 4000 ms. */
     int32_t wait_limit_ms;
-    int32_t reserved[5];
+    /* 3-way tensor engine: SNP rows of the Y-Z pair table held in device
+     * memory at once (rounded up to a multiple of 128).  0 = automatic: the
+     * whole table (32 x num_snps^2 bytes) when it fits beside the engine's
+     * other buffers, else the largest block that fits; the search then runs
+     * one pass per block of second SNPs Y (as the reference keeps its pair
+     * counts per 256-SNP Y block, src/search-triplets.cu:173-176), with the
+     * same results. */
+    int32_t pair_block_snps;
+    int32_t reserved[4];
 } episdet_options;
 
 typedef struct episdet_result {

@@ -424,6 +424,7 @@ episdet_status check_options(const episdet_options* in, int M, episdet_options* 
     if (o->top_k > kMaxTopK) return set_error(EPISDET_ERR_INVALID_ARGUMENT, "top_k must be <= %d", kMaxTopK);
     if (o->engine < EPISDET_ENGINE_AUTO || o->engine > EPISDET_ENGINE_SIMT)
         return set_error(EPISDET_ERR_INVALID_ARGUMENT, "unknown engine %d", o->engine);
+    if (o->pair_block_snps < 0) return set_error(EPISDET_ERR_INVALID_ARGUMENT, "pair_block_snps must be >= 0");
     if (o->first_end <= 0 || o->first_end > M) o->first_end = M;
     if (o->first_begin < 0 || o->first_begin >= o->first_end)
         return set_error(EPISDET_ERR_INVALID_ARGUMENT, "empty first-SNP slab [%d,%d)", o->first_begin, o->first_end);

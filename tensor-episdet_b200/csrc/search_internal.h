@@ -54,6 +54,7 @@ struct Workspace {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     std::mutex mu;
     DevBuf bits[2], marg[2], pair4[2], t32, t64, slots, counts, tiles, merged, mcount, fp64, flag;
+    DevBuf pairx[2];      // 3-way tensor engine, Y-blocked pair table: pair rows of the current first SNPs
     DevBuf planes8;       // unpacked 0/1 byte operand rows (tensor engine)
     DevBuf xsub[kXSets * kXGroup];  // per-X sample-regrouped operand rows (tensor engine)
     DevBuf xinfo;         // per-X segment tables (tensor engine)
@@ -77,7 +78,8 @@ struct Workspace {
 
     void release_all() {
         for (DevBuf& b : xsub) b.release();
-        DevBuf* all[] = {&bits[0], &bits[1], &marg[0], &marg[1], &pair4[0], &pair4[1], &t32, &t64, &slots,
+        DevBuf* all[] = {&bits[0], &bits[1], &marg[0], &marg[1], &pair4[0], &pair4[1], &pairx[0], &pairx[1], &t32,
+                         &t64, &slots,
                          &counts, &tiles, &merged, &mcount, &fp64, &flag, &planes8, &xinfo,
                          &tensor_flag, &cbuf, &perm_tot, &perm_planes, &perm_cls[0], &perm_cls[1], &perm_idx,
                          &bin_geno, &bin_idx, &bin_out[0], &bin_out[1]};

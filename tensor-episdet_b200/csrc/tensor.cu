@@ -129,6 +129,18 @@ struct GroupDesc {
     const XInfo* xinfo;
 };
 
+// A window of the 3-way pair table: cells of pair (r, col) at
+// p[c][(r - r0) * ld + (col - c0)] for class c, rows r >= r0, columns col > r.
+struct PairView {
+    const uint4* p[2];
+    int r0, c0;
+    long ld;
+};
+
+__device__ __forceinline__ uint4 pair_at(const PairView& v, int c, int r, int col) {
+    return __ldg(v.p[c] + (size_t)(r - v.r0) * (size_t)v.ld + (size_t)(col - v.c0));
+}
+
 struct TcParams {
     DevData D;
     ScoreTables T;
@@ -141,6 +153,11 @@ struct TcParams {
     int first_begin, first_end;
     uint4* pair_out0;
     uint4* pair_out1;
+    int out_r0, out_c0;  // store mode: pair (r, col) at pair_out[(r - out_r0) * out_ld + (col - out_c0)]
+    long out_ld;
+    // Triplets: X-Y and X-Z cells from xv, Y-Z cells from yv (one view of the
+    // whole table, or a block of Y rows and the rows of the current X values).
+    PairView xv, yv;
     int* err;
     Cand* cbuf;        // kFeatGlobalCands instances: [grid][kCapG] candidate buffers in global memory
     // 2-way label mode: [M][M] AND cells of every pair over all samples of the
@@ -922,12 +939,17 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                 // While this tile's MMAs run, bring its Y-Z and X-Z pair-table
                 // rows into L2 (one row of 56 entries per thread and class).
                 const int bz0 = tl.y * C::kZSnps;
-                const int nz = min(C::kZSnps, M - bz0);
-                if (nz > 0 && etid < 2 * kTileSnps + 2) {
-                    const int c = etid < 2 * kTileSnps ? etid / kTileSnps : etid - 2 * kTileSnps;
-                    const int row = etid < 2 * kTileSnps ? tl.x * 2 * kTileSnps + rank * kTileSnps + etid % kTileSnps
-                                                         : s_grp[g].x;
-                    if (row < M) ptx::prefetch_l2(P.D.pair4[c] + (size_t)row * M + bz0, (uint32_t)nz * 16u);
+                if (etid < 2 * kTileSnps + 2) {
+                    const bool yrow = etid < 2 * kTileSnps;
+                    const int c = yrow ? etid / kTileSnps : etid - 2 * kTileSnps;
+                    const int row = yrow ? tl.x * 2 * kTileSnps + rank * kTileSnps + etid % kTileSnps : s_grp[g].x;
+                    const PairView& v = yrow ? P.yv : P.xv;
+                    // Columns past the row only (the view holds no others).
+                    const int z0 = max(bz0, row + 1);
+                    const int nz = min(bz0 + C::kZSnps, M) - z0;
+                    if (row < M && nz > 0)
+                        ptx::prefetch_l2(v.p[c] + (size_t)(row - v.r0) * (size_t)v.ld + (size_t)(z0 - v.c0),
+                                         (uint32_t)nz * 16u);
                 }
             }
             // The decision to leave must be uniform over the 256 epilogue
@@ -982,7 +1004,7 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
 #pragma unroll
                     for (int c = 0; c < 2; ++c) {
                         load_marg3(P.D.marg[c], M, X, mx[c]);
-                        pair9_from4(xy9[c], __ldg(P.D.pair4[c] + (size_t)X * M + arow), mx[c], ma[c]);
+                        pair9_from4(xy9[c], pair_at(P.xv, c, X, arow), mx[c], ma[c]);
                     }
                 }
             }
@@ -1051,7 +1073,8 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                     };
                     if (mode == kPairsStore) {
                         if (row_ok && arow < bsnp && bsnp < M) {
-                            size_t o = (size_t)arow * M + bsnp;
+                            const size_t o =
+                                (size_t)(arow - P.out_r0) * (size_t)P.out_ld + (size_t)(bsnp - P.out_c0);
                             P.pair_out0[o] = make_uint4(cnt(0, 0, 0), cnt(0, 0, 1), cnt(0, 1, 0), cnt(0, 1, 1));
                             if (P.pair_out1)
                                 P.pair_out1[o] = make_uint4(cnt(1, 0, 0), cnt(1, 0, 1), cnt(1, 1, 0), cnt(1, 1, 1));
@@ -1098,7 +1121,7 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                     for (int c = 0; c < 2; ++c) {
                         int mz[3], xz9[9], yz9[9];
                         load_marg3(P.D.marg[c], M, bsnp, mz);
-                        const uint4 yz = __ldg(P.D.pair4[c] + (size_t)arow * M + bsnp);
+                        const uint4 yz = pair_at(P.yv, c, arow, bsnp);
                         const int yz4[4] = {(int)yz.x, (int)yz.y, (int)yz.z, (int)yz.w};
 #pragma unroll
                         for (int jj = 0; jj < 2; ++jj)
@@ -1109,7 +1132,7 @@ __global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
                                 tab[c][EPI_C3(0, jj, kk)] = ga == 0 ? g0 : (gb == 0 ? g1 : gdv);
                                 tab[c][EPI_C3(1, jj, kk)] = ga == 1 ? g0 : (gb == 1 ? g1 : gdv);
                             }
-                        pair9_from4(xz9, __ldg(P.D.pair4[c] + (size_t)X * M + bsnp), mx[c], mz);
+                        pair9_from4(xz9, pair_at(P.xv, c, X, bsnp), mx[c], mz);
                         pair9_from4(yz9, yz, ma[c], mz);
                         derive27(tab[c], xy9[c], xz9, yz9);
                     }
@@ -1294,6 +1317,7 @@ episdet_status tensor_pair_totals(Workspace* w, const uint32_t* d_planes, int M,
     p.seg2[1] = Seg{Kc / kKB, Kc / kKB};
     p.pair_out0 = out;
     p.pair_out1 = nullptr;
+    p.out_ld = M;
     tc_kernel<false, false><<<std::max(1, std::min(w->sms, (int)ptiles.size())), kThreads,
                               KCfg<false, false>::kSmemTotal, w->st>>>(tm2, p);
     CHECK_LAUNCH();
@@ -1436,63 +1460,141 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     p.seg2[0] = Seg{0, Kc / kKB};
     p.seg2[1] = Seg{Kc / kKB, pitch2 / kKB};
 
-    // 3-way: pair table of every SNP pair whose first index is in a tile >= fb's.
-    for (int c = 0; c < 2; ++c) {
-        CUDA_TRY(w->pair4[c].ensure(sizeof(uint4) * (size_t)M * M));
-        D.pair4[c] = (const uint4*)w->pair4[c].p;
-    }
-    p.D = D;
-    std::vector<int2> ptiles;
-    for (int a = fb / kTileSnps; a < nt; ++a)
-        for (int b = a; b < nt; ++b) ptiles.push_back(make_int2(a, b));
-    // Triplet tile lists of the CTA-pair kernel, one per first A pair tile
-    // a0 = (X+1) / 128: every (A pair tile a of 128 SNPs, B tile b of 56 SNPs)
-    // with a0 <= a whose Z range reaches past the tile's first Y
-    // (b >= bfirst(a)), ordered in bands of about 768 x 784 SNPs so that a wave
-    // of concurrent tiles shares few A and B row panels in L2.
+    // 3-way pair table.  Whole: every pair whose first SNP lies in a tile >=
+    // fb's, an [M][M] window per class, filled once.  Y-blocked (when the
+    // whole table does not fit beside the other buffers, or as
+    // o.pair_block_snps asks): the rows of one block of second SNPs Y at a
+    // time ([BY][M - y0] from column y0), plus the rows of the current first
+    // SNPs X ([128][M - xt0]); the first SNPs are then swept once per Y block,
+    // each pass counting only the triplets whose Y lies in the block (the
+    // reference keeps [9][BLOCK_SIZE][M] pair counts per Y block,
+    // src/search-triplets.cu:173-176).
     const int nt2 = (M + 2 * kTileSnps - 1) / (2 * kTileSnps);
     const int ntb = (M + kZSnpsPair - 1) / kZSnpsPair;
     const int a_first = (fb + 1) / (2 * kTileSnps);
-    constexpr int kBandA = kBand / 2, kBandB = 14;
-    auto bfirst = [](int a) { return (2 * kTileSnps * a) / kZSnpsPair; };
-    std::vector<int2> lists;
-    std::vector<size_t> list_off((size_t)nt2 + 1, 0);
-    std::vector<int> list_len((size_t)nt2 + 1, 0);
-    for (int a0 = a_first; a0 < nt2; ++a0) {
-        list_off[a0] = lists.size();
-        for (int ba = a0; ba < nt2; ba += kBandA)
-            for (int bb = bfirst(ba); bb < ntb; bb += kBandB)
-                for (int a = ba; a < std::min(nt2, ba + kBandA); ++a)
-                    for (int b = std::max(bfirst(a), bb); b < std::min(ntb, bb + kBandB); ++b)
-                        lists.push_back(make_int2(a, b));
-        list_len[a0] = (int)(lists.size() - list_off[a0]);
-    }
-    CUDA_TRY(w->tiles.ensure(sizeof(int2) * (ptiles.size() + lists.size())));
-    int2* d_ptiles = (int2*)w->tiles.p;
-    int2* d_lists = d_ptiles + ptiles.size();
-    CUDA_TRY(cudaMemcpyAsync(d_ptiles, ptiles.data(), sizeof(int2) * ptiles.size(), cudaMemcpyHostToDevice, w->st));
-    CUDA_TRY(cudaMemcpyAsync(d_lists, lists.data(), sizeof(int2) * lists.size(), cudaMemcpyHostToDevice, w->st));
-    w->h2d += (int64_t)(sizeof(int2) * (ptiles.size() + lists.size()));
-    p.ngroup = 1;
-    p.grp[0] = GroupDesc{d_ptiles, 0, -1, nullptr};
-    p.ntiles = (int)ptiles.size();
-    p.mode = kPairsStore;
-    p.pair_out0 = (uint4*)w->pair4[0].p;
-    p.pair_out1 = (uint4*)w->pair4[1].p;
-    tc_kernel<false, false><<<std::max(1, std::min(grid, (int)ptiles.size())), kThreads, KCfg<false, false>::kSmemTotal, w->st>>>(tm2,
-                                                                                                               p);
-    CHECK_LAUNCH();
-    ++*launches;
-
-    // Regrouped operands of the kMaxGroup X values of a launch, and their segment tables.
+    const int xend = std::min(fe, M - 2);
     // Regrouped rows: both classes' packed e2m1 regions, 2 samples per byte.
     const int pitchx = (Kc + kClassPad) / 2 + (Kn + kClassPad) / 2;
     const int max_n = std::max(D.n[0], D.n[1]);
+    const size_t info_bytes = 256;
+    const size_t idx_bytes = sizeof(int) * 4 * (size_t)max_n;
+    int blk_tiles = nt2 - a_first;  // A pair tiles (128 Y SNPs) per Y block
+    {
+        const size_t row_bytes = 2 * sizeof(uint4) * (size_t)M;  // one table row, both classes
+        const size_t xrows_bytes = row_bytes * 2 * kTileSnps;
+        size_t other = (size_t)rows * pitch2 + (size_t)kXSets * kMaxGroup * rows * pitchx +
+                       (size_t)kXSets * kMaxGroup * (info_bytes + idx_bytes) + sizeof(Cand) * (size_t)kCapG * grid;
+        // Buffers this workspace already holds are reused (or replaced) below.
+        size_t held = w->pair4[0].cap + w->pair4[1].cap + w->pairx[0].cap + w->pairx[1].cap + w->planes8.cap +
+                      w->xinfo.cap + w->cbuf.cap;
+        for (const DevBuf& b : w->xsub) held += b.cap;
+        size_t fr = 0, tot = 0;
+        CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+        // Left for the tile lists, slots, merge buffers and the driver.
+        const size_t reserve = std::max<size_t>(tot / 32, (size_t)1 << 30);
+        const size_t avail = fr + held > reserve ? fr + held - reserve : 0;
+        if (o.pair_block_snps > 0) {
+            blk_tiles = std::min(blk_tiles, (o.pair_block_snps + 2 * kTileSnps - 1) / (2 * kTileSnps));
+        } else if (row_bytes * (size_t)M + other > avail) {
+            const size_t left = avail > other + xrows_bytes ? avail - other - xrows_bytes : 0;
+            blk_tiles = (int)std::min<size_t>((size_t)blk_tiles, left / (row_bytes * 2 * kTileSnps));
+            if (blk_tiles < 1)
+                return set_error(EPISDET_ERR_OUT_OF_MEMORY,
+                                 "3-way search of %d SNPs: no 128-row block of the pair table fits beside the "
+                                 "%.1f GB of operand buffers",
+                                 M, (double)other / 1e9);
+        }
+    }
+    const bool blocked = blk_tiles < nt2 - a_first;
+    const int nblk = (nt2 - a_first + blk_tiles - 1) / blk_tiles;
+    for (int c = 0; c < 2; ++c) {
+        if (blocked) {
+            CUDA_TRY(w->pair4[c].ensure(sizeof(uint4) * (size_t)blk_tiles * 2 * kTileSnps * M));
+            CUDA_TRY(w->pairx[c].ensure(sizeof(uint4) * (size_t)2 * kTileSnps * M));
+        } else {
+            CUDA_TRY(w->pair4[c].ensure(sizeof(uint4) * (size_t)M * M));
+        }
+        D.pair4[c] = (const uint4*)w->pair4[c].p;
+    }
+    p.D = D;
+    // Pair-table tile list: every 64-SNP tile pair (a, b >= a) in order of a,
+    // so that the tiles of rows [64 a_lo, 64 a_hi) are one sub-range.
+    std::vector<int2> tri;
+    std::vector<size_t> tri_off((size_t)nt + 1, 0);
+    for (int a = 0; a < nt; ++a) {
+        tri_off[a] = tri.size();
+        for (int b = a; b < nt; ++b) tri.push_back(make_int2(a, b));
+    }
+    tri_off[nt] = tri.size();
+    // Triplet tile lists, one per (Y block, first A pair tile a0 = (X+1)/128):
+    // every (A pair tile a of 128 Y SNPs, B tile b of 56 Z SNPs) with
+    // max(a0, first tile of the block) <= a < end of the block, whose Z range
+    // reaches past the tile's first Y (b >= bfirst(a)), ordered in bands of
+    // about 768 x 784 SNPs so that a wave of concurrent tiles shares few A and
+    // B row panels in L2.  First SNPs below the block share one list; lists
+    // are built only for the first SNPs of this call's slab.
+    constexpr int kBandA = kBand / 2, kBandB = 14;
+    auto bfirst = [](int a) { return (2 * kTileSnps * a) / kZSnpsPair; };
+    const int a_last = std::min(nt2 - 1, xend / (2 * kTileSnps));  // a0 of the slab's last first SNP
+    std::vector<int2> lists;
+    std::vector<size_t> list_off((size_t)nblk * (nt2 + 1), 0);
+    std::vector<int> list_len((size_t)nblk * (nt2 + 1), 0);
+    for (int blk = 0; blk < nblk; ++blk) {
+        const int ya0 = a_first + blk * blk_tiles, ya1 = std::min(nt2, ya0 + blk_tiles);
+        for (int a0 = a_first; a0 < std::min(ya1, a_last + 1); ++a0) {
+            const size_t li = (size_t)blk * (nt2 + 1) + a0;
+            if (a0 < ya0 && a0 > a_first) {  // same list as the block's first a0
+                list_off[li] = list_off[li - 1];
+                list_len[li] = list_len[li - 1];
+                continue;
+            }
+            list_off[li] = lists.size();
+            for (int ba = std::max(a0, ya0); ba < ya1; ba += kBandA)
+                for (int bb = bfirst(ba); bb < ntb; bb += kBandB)
+                    for (int a = ba; a < std::min(ya1, ba + kBandA); ++a)
+                        for (int b = std::max(bfirst(a), bb); b < std::min(ntb, bb + kBandB); ++b)
+                            lists.push_back(make_int2(a, b));
+            list_len[li] = (int)(lists.size() - list_off[li]);
+        }
+    }
+    CUDA_TRY(w->tiles.ensure(sizeof(int2) * (tri.size() + lists.size())));
+    int2* d_tri = (int2*)w->tiles.p;
+    int2* d_lists = d_tri + tri.size();
+    CUDA_TRY(cudaMemcpyAsync(d_tri, tri.data(), sizeof(int2) * tri.size(), cudaMemcpyHostToDevice, w->st));
+    CUDA_TRY(cudaMemcpyAsync(d_lists, lists.data(), sizeof(int2) * lists.size(), cudaMemcpyHostToDevice, w->st));
+    w->h2d += (int64_t)(sizeof(int2) * (tri.size() + lists.size()));
+    // Counts of the pairs of SNP rows [r0, r1) (tile-aligned r0) with every
+    // later SNP, stored at (row - r0) * (M - r0) + (col - r0) of out (or at
+    // row * M + col when whole).
+    auto store_pairs = [&](uint4* out0, uint4* out1, int r0, int r1, bool whole) -> episdet_status {
+        const int t0 = r0 / kTileSnps, t1 = std::min(nt, (r1 + kTileSnps - 1) / kTileSnps);
+        const int n = (int)(tri_off[t1] - tri_off[t0]);
+        p.ngroup = 1;
+        p.grp[0] = GroupDesc{d_tri + tri_off[t0], 0, -1, nullptr};
+        p.ntiles = n;
+        p.mode = kPairsStore;
+        p.pair_out0 = out0;
+        p.pair_out1 = out1;
+        p.out_r0 = whole ? 0 : r0;
+        p.out_c0 = whole ? 0 : r0;
+        p.out_ld = whole ? M : M - r0;
+        tc_kernel<false, false><<<std::max(1, std::min(grid, n)), kThreads, KCfg<false, false>::kSmemTotal, w->st>>>(
+            tm2, p);
+        CHECK_LAUNCH();
+        ++*launches;
+        return EPISDET_OK;
+    };
+    if (!blocked) {
+        st = store_pairs((uint4*)w->pair4[0].p, (uint4*)w->pair4[1].p, fb / kTileSnps * kTileSnps, M, true);
+        if (st != EPISDET_OK) return st;
+        p.xv = PairView{{D.pair4[0], D.pair4[1]}, 0, 0, M};
+        p.yv = p.xv;
+    }
+
+    // Regrouped operands of the kMaxGroup X values of a launch, and their segment tables.
     for (int i = 0; i < kXSets * kMaxGroup; ++i) CUDA_TRY(w->xsub[i].ensure((size_t)rows * pitchx));
     // kXSets sets of regrouped operands and segment tables: the regrouping of
     // the next groups (on aux_st) overlaps the counting launch of group g (on st).
-    const size_t info_bytes = 256;
-    const size_t idx_bytes = sizeof(int) * 4 * (size_t)max_n;
     CUDA_TRY(w->xinfo.ensure(kXSets * kMaxGroup * (info_bytes + idx_bytes)));
     TmapPack tmx[kXSets];
     XInfo* d_info[kXSets][kMaxGroup];
@@ -1515,7 +1617,6 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
             co[b].row0[i] = 0;
         }
     }
-    const int xend = std::min(fe, M - 2);
     p.mode = kTriplets;
     CUDA_TRY(w->cbuf.ensure(sizeof(Cand) * (size_t)kCapG * grid));
     p.cbuf = (Cand*)w->cbuf.p;
@@ -1558,54 +1659,82 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     // The regrouping reads the planes and marginals staged on st.
     CUDA_TRY(cudaEventRecord(w->ev_ready, w->st));
     CUDA_TRY(cudaStreamWaitEvent(w->aux_st, w->ev_ready, 0));
+    // Pair tiles each first SNP was counted against (for the MAC count).
+    std::vector<double> x_tiles(w->timing ? (size_t)M : 0, 0.0);
     int gi = 0;
-    for (int x0 = fb; x0 < xend; x0 += kMaxGroup, ++gi) {
-        const int gn = std::min(kMaxGroup, xend - x0);
-        const int b = gi % kXSets;
-        // Index lists and regrouped rows of the gn first SNPs, one launch each,
-        // into buffer set b once the counting launch that last read it is done.
-        if (gi >= kXSets) CUDA_TRY(cudaStreamWaitEvent(w->aux_st, w->ev_tc[b], 0));
-        xw[b].x0 = x0;
-        xinfo_kernel<<<dim3(2, gn), kXinfoThreads, 0, w->aux_st>>>(D, xw[b]);
-        CHECK_LAUNCH();
-        for (int g = 0; g < gn; ++g) co[b].row0[g] = kNPair * bfirst((x0 + g + 1) / (2 * kTileSnps));
-        const int max_rows = rows - co[b].row0[0];  // the first member needs the most rows
-        const dim3 cgrid(cmp_chunks(D.W[0]) + cmp_chunks(D.W[1]), (max_rows + kCmpRows - 1) / kCmpRows, gn);
-        compact_kernel<<<cgrid, kCmpThreads, 0, w->aux_st>>>(D, xw[b], co[b], rows, pitchx);
-        CHECK_LAUNCH();
-        CUDA_TRY(cudaEventRecord(w->ev_cmp[b], w->aux_st));
-        CUDA_TRY(cudaStreamWaitEvent(w->st, w->ev_cmp[b], 0));
-        *launches += 2;
-        int cum = 0;
-        for (int g = 0; g < gn; ++g) {
-            const int x = x0 + g;
-            if (progress && x % 256 == 0) printf("Outer loop iteration %d out of %d\n", x / 256, bs_lines);
-            const int a0 = (x + 1) / (2 * kTileSnps);
-            p.grp[g] = GroupDesc{d_lists + list_off[a0], cum, x, d_info[b][g]};
-            cum += list_len[a0];
+    int xt0 = -1;  // first row held in pairx (Y-blocked)
+    for (int blk = 0; blk < nblk; ++blk) {
+        const int ya0 = a_first + blk * blk_tiles, ya1 = std::min(nt2, ya0 + blk_tiles);
+        const int y0 = ya0 * 2 * kTileSnps, y1 = std::min(M, ya1 * 2 * kTileSnps);
+        if (blocked) {
+            // Y-Z rows of this block (the previous block's launches, on the
+            // same stream, have read theirs).
+            st = store_pairs((uint4*)w->pair4[0].p, (uint4*)w->pair4[1].p, y0, y1, false);
+            if (st != EPISDET_OK) return st;
+            p.yv = PairView{{D.pair4[0], D.pair4[1]}, y0, y0, M - y0};
         }
-        p.ngroup = gn;
-        p.ntiles = cum;
-        CUDA_TRY(timer_begin(w));
-        {
-            cudaLaunchConfig_t cfg = {};
-            cudaLaunchAttribute attr[1];
-            attr[0].id = cudaLaunchAttributeClusterDimension;
-            attr[0].val.clusterDim.x = 2;
-            attr[0].val.clusterDim.y = 1;
-            attr[0].val.clusterDim.z = 1;
-            cfg.gridDim = dim3(2 * std::max(1, std::min(pairs, cum)), 1, 1);
-            cfg.blockDim = dim3(kThreads, 1, 1);
-            cfg.dynamicSmemBytes = ksmem;
-            cfg.stream = w->st;
-            cfg.attrs = attr;
-            cfg.numAttrs = 1;
-            CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, tmx[b], p));
+        const int xe = std::min(xend, y1 - 1);  // X < Y < y1
+        for (int x0 = fb; x0 < xe; x0 += kMaxGroup) {
+            const int gn = std::min(kMaxGroup, xe - x0);
+            const int b = gi % kXSets;
+            int cum = 0;
+            for (int g = 0; g < gn; ++g) {
+                const int x = x0 + g;
+                if (progress && x % 256 == 0 && x + 1 >= y0) printf("Outer loop iteration %d out of %d\n", x / 256, bs_lines);
+                const size_t li = (size_t)blk * (nt2 + 1) + (x + 1) / (2 * kTileSnps);
+                p.grp[g] = GroupDesc{d_lists + list_off[li], cum, x, d_info[b][g]};
+                cum += list_len[li];
+                if (w->timing) x_tiles[x] += list_len[li];
+            }
+            if (cum == 0) continue;
+            ++gi;
+            if (blocked && (xt0 < 0 || x0 < xt0 || x0 + gn > xt0 + 2 * kTileSnps)) {
+                // X-Y and X-Z rows of this group's first SNPs (and the next ones').
+                xt0 = x0 / kTileSnps * kTileSnps;
+                st = store_pairs((uint4*)w->pairx[0].p, (uint4*)w->pairx[1].p, xt0, std::min(M, xt0 + 2 * kTileSnps),
+                                 false);
+                if (st != EPISDET_OK) return st;
+                p.xv = PairView{{(const uint4*)w->pairx[0].p, (const uint4*)w->pairx[1].p}, xt0, xt0, M - xt0};
+            }
+            // Index lists and regrouped rows of the gn first SNPs, one launch each,
+            // into buffer set b once the counting launch that last read it is done.
+            if (gi > kXSets) CUDA_TRY(cudaStreamWaitEvent(w->aux_st, w->ev_tc[b], 0));
+            xw[b].x0 = x0;
+            xinfo_kernel<<<dim3(2, gn), kXinfoThreads, 0, w->aux_st>>>(D, xw[b]);
+            CHECK_LAUNCH();
+            for (int g = 0; g < gn; ++g)
+                co[b].row0[g] = kNPair * bfirst(std::max((x0 + g + 1) / (2 * kTileSnps), ya0));
+            const int max_rows = rows - co[b].row0[0];  // the first member needs the most rows
+            const dim3 cgrid(cmp_chunks(D.W[0]) + cmp_chunks(D.W[1]), (max_rows + kCmpRows - 1) / kCmpRows, gn);
+            compact_kernel<<<cgrid, kCmpThreads, 0, w->aux_st>>>(D, xw[b], co[b], rows, pitchx);
+            CHECK_LAUNCH();
+            CUDA_TRY(cudaEventRecord(w->ev_cmp[b], w->aux_st));
+            CUDA_TRY(cudaStreamWaitEvent(w->st, w->ev_cmp[b], 0));
+            *launches += 2;
+            p.ngroup = gn;
+            p.ntiles = cum;
+            p.mode = kTriplets;
+            CUDA_TRY(timer_begin(w));
+            {
+                cudaLaunchConfig_t cfg = {};
+                cudaLaunchAttribute attr[1];
+                attr[0].id = cudaLaunchAttributeClusterDimension;
+                attr[0].val.clusterDim.x = 2;
+                attr[0].val.clusterDim.y = 1;
+                attr[0].val.clusterDim.z = 1;
+                cfg.gridDim = dim3(2 * std::max(1, std::min(pairs, cum)), 1, 1);
+                cfg.blockDim = dim3(kThreads, 1, 1);
+                cfg.dynamicSmemBytes = ksmem;
+                cfg.stream = w->st;
+                cfg.attrs = attr;
+                cfg.numAttrs = 1;
+                CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, tmx[b], p));
+            }
+            CHECK_LAUNCH();
+            CUDA_TRY(timer_end(w));
+            CUDA_TRY(cudaEventRecord(w->ev_tc[b], w->st));
+            *launches += 1;
         }
-        CHECK_LAUNCH();
-        CUDA_TRY(timer_end(w));
-        CUDA_TRY(cudaEventRecord(w->ev_tc[b], w->st));
-        *launches += 1;
     }
     if (w->timing) {
         // Tensor MACs issued: per X, pair tiles x 256 x 112 x the regrouped K extent,
@@ -1628,8 +1757,7 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
             for (int c = 0; c < 2; ++c)
                 for (int g = 0; g < 3; ++g)
                     if (g != gd) kext += ((mg[c][(size_t)g * M + x] + kF4PerKB - 1) / kF4PerKB) * (long)kF4PerKB;
-            const int a0 = (x + 1) / (2 * kTileSnps);
-            macs += (double)list_len[a0] * 2 * kTileRows * kNPair * (double)kext;
+            macs += x_tiles[x] * 2 * kTileRows * kNPair * (double)kext;
         }
         w->executed_macs = macs;
     }

@@ -73,7 +73,8 @@ class Options(ctypes.Structure):
     _fields_ = [("order", ctypes.c_int32), ("score", ctypes.c_int32), ("top_k", ctypes.c_int32),
                 ("device", ctypes.c_int32), ("engine", ctypes.c_int32), ("first_begin", ctypes.c_int32),
                 ("first_end", ctypes.c_int32), ("flags", ctypes.c_uint32), ("stream", ctypes.c_uint64),
-                ("wait_limit_ms", ctypes.c_int32), ("reserved", ctypes.c_int32 * 5)]
+                ("wait_limit_ms", ctypes.c_int32), ("pair_block_snps", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 4)]
 
 
 class Result(ctypes.Structure):
@@ -294,7 +295,7 @@ def _ptr(a):
 
 
 def make_options(order=3, score="k2", top_k=1024, device=0, engine="auto", first_begin=0, first_end=0,
-                 flags=0, stream=0, wait_limit_ms=0) -> Options:
+                 flags=0, stream=0, wait_limit_ms=0, pair_block_snps=0) -> Options:
     o = Options()
     lib().episdet_default_options(ctypes.byref(o))
     o.order = order
@@ -306,6 +307,7 @@ def make_options(order=3, score="k2", top_k=1024, device=0, engine="auto", first
     o.first_begin, o.first_end, o.flags = first_begin, first_end, flags
     o.stream = int(stream)
     o.wait_limit_ms = int(wait_limit_ms)
+    o.pair_block_snps = int(pair_block_snps)
     return o
 
 
@@ -332,7 +334,7 @@ def _to_result(order: int, r: Result, bufs) -> SearchResult:
 
 def search(cases, controls, num_cases: int, num_controls: int, *, num_snps: Optional[int] = None, order: int = 3,
            score="k2", top_k: int = 1024, device: int = 0, engine="auto", first_begin: int = 0, first_end: int = 0,
-           flags: int = 0, stream: int = 0, wait_limit_ms: int = 0) -> SearchResult:
+           flags: int = 0, stream: int = 0, wait_limit_ms: int = 0, pair_block_snps: int = 0) -> SearchResult:
     """Exhaustive search; cases/controls are host uint32 arrays or CUDA tensors in the plane format."""
     pc, mc = _ptr(cases)
     pn, mn = _ptr(controls)
@@ -340,7 +342,8 @@ def search(cases, controls, num_cases: int, num_controls: int, *, num_snps: Opti
         raise TypeError("cases and controls must live in the same memory")
     M = num_snps if num_snps is not None else int(cases.shape[0])
     d = Dataset(pc, pn, M, num_cases, num_controls, mc)
-    o = make_options(order, score, top_k, device, engine, first_begin, first_end, flags, stream, wait_limit_ms)
+    o = make_options(order, score, top_k, device, engine, first_begin, first_end, flags, stream, wait_limit_ms,
+                     pair_block_snps)
     r, bufs = _result_buffers(top_k)
     _check(lib().episdet_search(ctypes.byref(d), ctypes.byref(o), ctypes.byref(r)))
     return _to_result(order, r, bufs)
