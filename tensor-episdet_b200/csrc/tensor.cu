@@ -1677,12 +1677,14 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
         for (int x0 = fb; x0 < xe; x0 += kMaxGroup) {
             const int gn = std::min(kMaxGroup, xe - x0);
             const int b = gi % kXSets;
+            // (Kept aside until the launch: store_pairs below rewrites p.grp.)
+            GroupDesc gdesc[kMaxGroup];
             int cum = 0;
             for (int g = 0; g < gn; ++g) {
                 const int x = x0 + g;
                 if (progress && x % 256 == 0 && x + 1 >= y0) printf("Outer loop iteration %d out of %d\n", x / 256, bs_lines);
                 const size_t li = (size_t)blk * (nt2 + 1) + (x + 1) / (2 * kTileSnps);
-                p.grp[g] = GroupDesc{d_lists + list_off[li], cum, x, d_info[b][g]};
+                gdesc[g] = GroupDesc{d_lists + list_off[li], cum, x, d_info[b][g]};
                 cum += list_len[li];
                 if (w->timing) x_tiles[x] += list_len[li];
             }
@@ -1711,6 +1713,10 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
             CUDA_TRY(cudaEventRecord(w->ev_cmp[b], w->aux_st));
             CUDA_TRY(cudaStreamWaitEvent(w->st, w->ev_cmp[b], 0));
             *launches += 2;
+            for (int g = 0; g < gn; ++g) {
+                if (gdesc[g].x < 0 || !gdesc[g].xinfo) return set_error(EPISDET_ERR_INTERNAL, "triplet group %d unset", g);
+                p.grp[g] = gdesc[g];
+            }
             p.ngroup = gn;
             p.ntiles = cum;
             p.mode = kTriplets;
