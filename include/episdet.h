@@ -282,6 +282,13 @@ int32_t episdet_abi_version(void);
 /* Frees the per-device workspace the library keeps between calls. */
 episdet_status episdet_release_workspace(int32_t device);
 
+/* Profiling aid -- no counterpart in the reference: after an episdet_search
+ * with EPISDET_FLAG_TIMING on `device`, the device time (ms, CUDA events on
+ * the launching stream) and the tensor MACs issued of each counting launch, in
+ * launch order (at most cap entries each; either pointer may be NULL).
+ * Returns the number of counting launches of that search (0 without the flag). */
+int64_t episdet_last_launch_profile(int32_t device, double* ms, double* macs, int64_t cap);
+
 /* Testing aid for failure detection -- no counterpart in the reference: the
  * after-th device allocation the library makes from now on (in any thread)
  * fails as if the device were out of memory, once; the call that needed it

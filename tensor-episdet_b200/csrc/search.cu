@@ -125,6 +125,8 @@ void begin_call(Workspace* w, const episdet_options& o) {
     w->tev_used = 0;
     w->count_launches = 0;
     w->executed_macs = 0.0;
+    w->launch_ms.clear();
+    w->launch_macs.clear();
 }
 
 cudaError_t timer_begin(Workspace* w) {
@@ -627,8 +629,12 @@ episdet_status search_locked(Workspace* w, const episdet_dataset* data, const ep
             float t = 0.0f;
             CUDA_TRY(cudaEventElapsedTime(&t, w->tev[i], w->tev[i + 1]));
             sum += t;
+            w->launch_ms.push_back(t);
         }
         result->count_kernel_ms = sum;
+        // A one-launch search (pairs, SIMT) issues all its MACs in that launch.
+        if (w->launch_macs.size() != w->launch_ms.size())
+            w->launch_macs.assign(w->launch_ms.size(), w->launch_ms.size() == 1 ? w->executed_macs : 0.0);
     }
     result->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return EPISDET_OK;
@@ -685,6 +691,23 @@ extern "C" episdet_status episdet_release_workspace(int32_t device) {
         w->release_all();
     }
     return EPISDET_OK;
+}
+
+extern "C" int64_t episdet_last_launch_profile(int32_t device, double* ms, double* macs, int64_t cap) {
+    if (device < 0 || device >= 64) return 0;
+    Workspace* w = nullptr;
+    {
+        std::lock_guard<std::mutex> g(g_ws_mu);
+        w = g_ws[device][0];
+    }
+    if (!w) return 0;
+    std::lock_guard<std::mutex> l(w->mu);
+    const int64_t n = (int64_t)w->launch_ms.size();
+    for (int64_t i = 0; i < std::min(n, cap); ++i) {
+        if (ms) ms[i] = w->launch_ms[(size_t)i];
+        if (macs) macs[i] = i < (int64_t)w->launch_macs.size() ? w->launch_macs[(size_t)i] : 0.0;
+    }
+    return n;
 }
 
 extern "C" void episdet_test_fail_allocation(int32_t after) { episdet::g_fail_alloc.store(after > 0 ? after : 0); }

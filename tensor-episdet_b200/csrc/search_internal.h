@@ -56,6 +56,7 @@ struct Workspace {
     DevBuf bits[2], marg[2], pair4[2], t32, t64, slots, counts, tiles, merged, mcount, fp64, flag;
     DevBuf pairx[2];      // 3-way tensor engine, Y-blocked pair table: pair rows of the current first SNPs
     DevBuf planes8;       // unpacked 0/1 byte operand rows (tensor engine)
+    DevBuf planes_t[2];   // sample-major transposed planes per class (3-way tensor engine's regrouping)
     DevBuf xsub[kXSets * kXGroup];  // per-X sample-regrouped operand rows (tensor engine)
     DevBuf xinfo;         // per-X segment tables (tensor engine)
     DevBuf tensor_flag;   // device error / progress words of the tensor engine
@@ -71,6 +72,7 @@ struct Workspace {
     int tev_used = 0;
     int64_t count_launches = 0;
     double executed_macs = 0.0;
+    std::vector<double> launch_ms, launch_macs;  // EPISDET_FLAG_TIMING: per counting launch of the last call
     int tab_score = -1, tab_nc = -1, tab_nn = -1;
     int stage_override = -1;  // triplet instance: -1 by the class-size rule, 0 plain, 1 staged
     float inv32 = 0.0f, hy32 = 0.0f, k2_margin = 0.0f;
@@ -80,7 +82,8 @@ struct Workspace {
         for (DevBuf& b : xsub) b.release();
         DevBuf* all[] = {&bits[0], &bits[1], &marg[0], &marg[1], &pair4[0], &pair4[1], &pairx[0], &pairx[1], &t32,
                          &t64, &slots,
-                         &counts, &tiles, &merged, &mcount, &fp64, &flag, &planes8, &xinfo,
+                         &counts, &tiles, &merged, &mcount, &fp64, &flag, &planes8, &planes_t[0], &planes_t[1],
+                         &xinfo,
                          &tensor_flag, &cbuf, &perm_tot, &perm_planes, &perm_cls[0], &perm_cls[1], &perm_idx,
                          &bin_geno, &bin_idx, &bin_out[0], &bin_out[1]};
         for (DevBuf* b : all) b->release();

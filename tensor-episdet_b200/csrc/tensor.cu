@@ -27,7 +27,7 @@
 //   triplets: segments {cases, controls} x {X genotype a, X genotype b}
 //                                                        -> 4 x 112 columns, one set
 // For triplets the sample columns are regrouped per first SNP X by X's
-// genotype (xinfo/compact kernels below), keeping the two genotypes of X with
+// genotype (xinfo/transpose/regroup kernels below), keeping the two genotypes of X with
 // the fewest samples; the third is recovered from the Y-Z pair table exactly
 // as the reference recovers genotype 2 (src/helper.cu:494-548).  This replaces
 // the materialised X AND Y operand of src/helper.cu:396-425 and reduces the
@@ -446,33 +446,6 @@ __global__ void __launch_bounds__(kXinfoThreads) xinfo_kernel(DevData D, XWork x
 // nibble (zero past the segment's length up to its 256-sample end).  Rows
 // below row0 are not needed by X.
 //
-// Output-stationary: a CTA owns kCmpOut output samples of one class region
-// (the two segments back to back) for kCmpRows rows.  Each thread keeps the
-// source sample indices of its 16 output samples (8 bytes) in registers and
-// reuses them for every row.  The source words those samples fall in (one
-// contiguous span per row) are copied into a ring of kCmpDepth shared-memory
-// buffers with cp.async, kCmpDepth - 1 rows ahead of the row being gathered.
-// Spans wider than kCmpSpanWords (first SNPs whose kept genotypes are rare)
-// gather from global memory.  The kernel is small (128 threads, 64 registers,
-// 4 KB of shared memory) so that its CTAs fit on the SMs beside the counting
-// CTAs: it runs on an auxiliary stream while the previous group is counted.
-constexpr int kCmpOut = 2048;
-constexpr int kCmpThreads = 128;
-constexpr int kCmpRows = 32;
-constexpr int kCmpSpanWords = 512;
-constexpr int kCmpDepth = 2;
-
-__host__ __device__ inline int cmp_chunks(int words) { return (words * 32 + kClassPad + kCmpOut - 1) / kCmpOut; }
-
-__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(ptx::smem_u32(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
 // Output rows of the members of one launch: member m = blockIdx.z writes rows
 // [row0[m], nrows_total) of out[m].
 struct CmpOut {
@@ -480,109 +453,160 @@ struct CmpOut {
     int row0[kMaxGroup];
 };
 
-__global__ void __launch_bounds__(kCmpThreads, 8)
-    compact_kernel(DevData D, XWork xw, CmpOut co, int rows_total, int pitch) {
-    // One zero word after each span buffer: padding samples read it.
-    __shared__ __align__(16) uint32_t s_src[kCmpDepth][kCmpSpanWords + 4];
-    __shared__ int s_lo, s_hi;
+// ------------------------------------------------- sample-major regrouping
+// Gathering single bits of the plane rows costs about ten instructions per
+// output byte, and a kernel doing that beside the counting kernel slowed it by
+// 15 %.  Instead the planes are transposed once per search into sample-major
+// words (tt[c][s][q]: bit 31 - i is row 32 q + i at sample s), so that
+// gathering a sample is a 128-byte copy, and the gathered block is turned
+// back into rows by a 32 x 32 bit transpose in registers (five shuffle
+// stages).
+
+// 32 x 32 bit transpose across a warp: lane k returns the word whose bit
+// 31 - l is bit 31 - k of lane l's word (the block-swap transpose of
+// H. S. Warren, Hacker's Delight, 2nd ed., section 7-3, one stage per
+// shuffle distance).
+__device__ __forceinline__ uint32_t warp_transpose32(uint32_t a, int lane) {
+    uint32_t m = 0x0000FFFFu;
+#pragma unroll
+    for (int j = 16; j != 0; j >>= 1, m ^= m << j) {
+        const uint32_t p = __shfl_xor_sync(0xFFFFFFFFu, a, j);
+        if (lane & j) {
+            a ^= ((p ^ (a >> j)) & m) << j;
+        } else {
+            a ^= (a ^ (p >> j)) & m;
+        }
+    }
+    return a;
+}
+
+// Rows padded to whole 256-row tiles in the sample-major layout.
+constexpr int kTtRows = 256;
+__host__ __device__ inline int tt_row_words(int rows) { return (rows + kTtRows - 1) / kTtRows * (kTtRows / 32); }
+
+// Planes of class c -> tt (one warp per 256 rows x 256 samples: eight
+// 32-byte reads of eight rows' words per lane, eight 32-byte writes).
+constexpr int kTtThreads = 256;
+__global__ void __launch_bounds__(kTtThreads) transpose_planes_kernel(DevData D, int c, uint32_t* __restrict__ tt,
+                                                                      int rows, int rwp) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (int)(blockIdx.x * (kTtThreads / 32) + threadIdx.x / 32);
+    const int W = D.W[c];
+    const int nqb = rwp / 8, nsb = W / 8;
+    if (warp >= nqb * nsb) return;  // uniform over the warp
+    const int qb = warp % nqb, sb = warp / nqb;
+    const uint32_t* __restrict__ bits = D.bits[c];
+    uint32_t out[8][8];  // [sample word][row word]
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int r = (qb * 8 + q) * 32 + lane;
+        uint4 v0 = make_uint4(0, 0, 0, 0), v1 = v0;
+        if (r < rows) {
+            const uint4* src = reinterpret_cast<const uint4*>(bits + (size_t)r * W + sb * 8);
+            v0 = __ldg(src);
+            v1 = __ldg(src + 1);
+        }
+        const uint32_t v[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
+#pragma unroll
+        for (int e = 0; e < 8; ++e) out[e][q] = warp_transpose32(v[e], lane);
+    }
+    // Lane k now holds, for sample 32 (sb*8 + e) + k, the words of rows
+    // 32 (qb*8 + q) .. + 31 (bit 31 - i = row 32 (qb*8 + q) + i).
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        uint4* dst = reinterpret_cast<uint4*>(tt + (size_t)((sb * 8 + e) * 32 + lane) * rwp + qb * 8);
+        dst[0] = make_uint4(out[e][0], out[e][1], out[e][2], out[e][3]);
+        dst[1] = make_uint4(out[e][4], out[e][5], out[e][6], out[e][7]);
+    }
+}
+
+// Regrouped operand rows for the members of one launch (the layout above),
+// from tt: a CTA covers kRgRows rows x 256 packed sample
+// positions (one K block) of one class region of one member.  Each thread
+// copies the 128 bytes of its position's source sample (these rows: one
+// cache line), then each warp turns 32 rows x 32 positions at a time back into
+// rows as e2m1 nibbles, collects the 128 bytes of each of its 32 rows in
+// shared memory and writes them as whole lines, 4 rows per store (a store of
+// 16 bytes into each of 32 rows a pitch apart ran at a third of the rate).
+// With 67 KB of shared memory its CTAs do not fit beside a counting CTA, so
+// they run on the SMs the previous counting launch has left.
+constexpr int kRgThreads = 256;
+constexpr int kRgRows = 1024;
+constexpr int kRgWords = kRgRows / 32;  // row words per position
+constexpr int kRgOutBytes = (kRgThreads / 32) * 32 * 8 * 16;
+constexpr int kRgTBytes = kRgThreads * (kRgWords + 1) * 4;
+constexpr int kRgSmem = kRgOutBytes + kRgTBytes + 256 * 4;
+__global__ void __launch_bounds__(kRgThreads, 2)
+    regroup_kernel(DevData D, XWork xw, CmpOut co, const uint32_t* __restrict__ tt0, const uint32_t* __restrict__ tt1,
+                   int rwp, int rows_total, int pitch) {
+    // Dynamic shared memory (kRgSmem bytes): per warp 32 rows x 8 chunks of 16
+    // bytes (chunk j of row r at slot j ^ (r & 7)); [position][row word],
+    // padded against bank conflicts; the nibble table.
+    extern __shared__ __align__(16) uint8_t rg_smem[];
+    uint4(*s_out)[32][8] = reinterpret_cast<uint4(*)[32][8]>(rg_smem);
+    uint32_t(*s_t)[kRgWords + 1] = reinterpret_cast<uint32_t(*)[kRgWords + 1]>(rg_smem + kRgOutBytes);
+    uint32_t* s_lut = reinterpret_cast<uint32_t*>(rg_smem + kRgOutBytes + kRgTBytes);
     const int mem = (int)blockIdx.z;
+    const int rt = (int)blockIdx.y;
+    const int row0 = co.row0[mem];
+    if ((rt + 1) * kRgRows <= row0 || rt * kRgRows >= rows_total) return;  // uniform over the CTA
     const XInfo* __restrict__ info = xw.info(mem);
-    const int* __restrict__ idx = xw.idx(mem);
-    const int max_n = xw.max_n;
-    const int row0 = co.row0[mem], nrows = rows_total - row0;
-    uint8_t* __restrict__ out = co.out[mem];
-    if ((int)blockIdx.y * kCmpRows >= nrows) return;  // uniform over the CTA
-    const int C0 = cmp_chunks(D.W[0]);
-    const int c = (int)blockIdx.x < C0 ? 0 : 1;
-    const int chunk = (int)blockIdx.x - (c ? C0 : 0);
+    const int T0 = (D.W[0] * 32 + kClassPad) / kF4PerKB;
+    const int c = (int)blockIdx.x < T0 ? 0 : 1;
+    const int k0 = ((int)blockIdx.x - (c ? T0 : 0)) * kF4PerKB;
     const int la = info->len[c][0], lb = info->len[c][1];
     const int pa = ((la + kF4PerKB - 1) / kF4PerKB) * kF4PerKB, pb = ((lb + kF4PerKB - 1) / kF4PerKB) * kF4PerKB;
-    const int region = pa + pb;
-    const int k0 = chunk * kCmpOut;
-    if (k0 >= region) return;  // uniform over the CTA
-    const int kk0 = k0 + 16 * (int)threadIdx.x;
-    const int* ia = idx + ((size_t)c * 2 + 0) * max_n;
-    const int* ib = idx + ((size_t)c * 2 + 1) * max_n;
-    int src[16];
-    int lo = 0x7FFFFFFF, hi = -1;
+    if (k0 >= pa + pb) return;  // uniform over the CTA
+    const int t = threadIdx.x;
+    // e2m1 nibbles of 8 positions (bit e of the index = position e): 1.0 = 2,
+    // the even position in the low nibble of each byte.
+    {
+        uint32_t v = 0;
 #pragma unroll
-    for (int e = 0; e < 16; ++e) {
-        const int k = kk0 + e;
-        int s = -1;
-        if (k < pa) {
-            if (k < la) s = __ldg(ia + k);
-        } else if (k < region) {
-            if (k - pa < lb) s = __ldg(ib + (k - pa));
-        }
-        src[e] = s;
-        if (s >= 0) {
-            lo = min(lo, s >> 5);
-            hi = max(hi, s >> 5);
-        }
+        for (int e = 0; e < 8; ++e) v |= ((t >> e) & 1u) << (4 * e + 1);
+        s_lut[t] = v;
     }
-    if (threadIdx.x == 0) {
-        s_lo = 0x7FFFFFFF;
-        s_hi = -1;
-        for (int d = 0; d < kCmpDepth; ++d) s_src[d][kCmpSpanWords] = 0u;
+    const int k = k0 + t;
+    const int* __restrict__ idx = xw.idx(mem) + (size_t)c * 2 * xw.max_n;
+    int src = -1;
+    if (k < pa) {
+        if (k < la) src = __ldg(idx + k);
+    } else if (k - pa < lb) {
+        src = __ldg(idx + xw.max_n + (k - pa));
+    }
+    // Row words past the padded row count (the last tile) read as zero.
+    const int nw = min(kRgWords, rwp - rt * kRgWords);
+    const uint4* p = reinterpret_cast<const uint4*>((c ? tt1 : tt0) + (size_t)max(src, 0) * rwp + rt * kRgWords);
+#pragma unroll
+    for (int e = 0; e < kRgWords / 4; ++e) {
+        const uint4 v = (src >= 0 && 4 * e < nw) ? __ldg(p + e) : make_uint4(0, 0, 0, 0);
+        s_t[t][4 * e] = v.x, s_t[t][4 * e + 1] = v.y, s_t[t][4 * e + 2] = v.z, s_t[t][4 * e + 3] = v.w;
     }
     __syncthreads();
-    if (hi >= 0) {
-        atomicMin(&s_lo, lo);
-        atomicMax(&s_hi, hi);
-    }
-    __syncthreads();
-    const int W = D.W[c];
-    // Span of source words, widened to whole 16-byte groups.  Rows are W words
-    // long with W a multiple of 32, so the widened span stays inside the row.
-    const int wlo = s_lo & ~3;
-    const int nq = s_hi >= s_lo ? (s_hi - wlo + 4) >> 2 : 0;  // 16-byte groups
-    const bool staged = nq > 0 && nq * 4 <= kCmpSpanWords;
-    const int colbase = ((c ? D.W[0] * 32 + kClassPad : 0) + kk0) / 2;  // byte of this thread's first sample
-    const int rbeg = row0 + (int)blockIdx.y * kCmpRows;
-    const int rend = min(row0 + nrows, rbeg + kCmpRows);
-    const uint32_t* base = D.bits[c];
-    if (staged) {
-        auto issue = [&](int row) {
-            if (row < rend) {
-                const uint32_t* srow = base + (size_t)row * W + wlo;
-                uint32_t* dst = s_src[(row - rbeg) % kCmpDepth];
-                for (int i = (int)threadIdx.x; i < nq; i += kCmpThreads) cp_async16(dst + 4 * i, srow + 4 * i);
-            }
-            cp_async_commit();  // one group per row, empty past the end
-        };
-        // Per sample, the same for every row: the word of the staged span
-        // (low 16 bits) and the bit's shift (high 16 bits).
-        uint32_t pk[16];
+    const int lane = t & 31, w = t >> 5;
+    const int colbase = ((c ? D.W[0] * 32 + kClassPad : 0) + k0) / 2;
+    uint4(*so)[8] = s_out[w];
+#pragma unroll 1
+    for (int q = w * (kRgWords / 8); q < (w + 1) * (kRgWords / 8); ++q) {
 #pragma unroll
-        for (int e = 0; e < 16; ++e) {
-            const int s = src[e];
-            pk[e] = s >= 0 ? (uint32_t)((s >> 5) - wlo) | ((uint32_t)(31 - (s & 31)) << 16) : (uint32_t)kCmpSpanWords;
+        for (int j = 0; j < kRgThreads / 32; ++j) {
+            // Lane l: row word q at position 32 j + l; after the transpose,
+            // lane k holds row 32 q + k with position 32 j + l at bit 31 - l.
+            const uint32_t x = __brev(warp_transpose32(s_t[32 * j + lane][q], lane));
+            so[lane][j ^ (lane & 7)] =
+                make_uint4(s_lut[x & 255u], s_lut[(x >> 8) & 255u], s_lut[(x >> 16) & 255u], s_lut[x >> 24]);
         }
+        __syncwarp();
+        // Store i: rows 4 i .. 4 i + 3 of the 32, eight lanes (16 bytes each) per row.
 #pragma unroll
-        for (int d = 0; d < kCmpDepth - 1; ++d) issue(rbeg + d);
-        for (int row = rbeg; row < rend; ++row) {
-            cp_async_wait<kCmpDepth - 2>();  // this thread's copies of `row` have landed
-            __syncthreads();                 // everyone's have, and the previous row's buffer is free
-            issue(row + kCmpDepth - 1);
-            const uint32_t* sw = s_src[(row - rbeg) % kCmpDepth];
-            uint32_t o[2] = {0, 0};
-#pragma unroll
-            for (int e = 0; e < 16; ++e)
-                o[e >> 3] |= ((sw[pk[e] & 0xFFFFu] >> (pk[e] >> 16)) & 1u) << (4 * (e & 7) + 1);
-            if (kk0 < region) *reinterpret_cast<uint2*>(out + (size_t)row * pitch + colbase) = make_uint2(o[0], o[1]);
+        for (int i = 0; i < 8; ++i) {
+            const int r = 4 * i + (lane >> 3), ch = lane & 7;
+            const int row = rt * kRgRows + q * 32 + r;
+            const uint4 o = so[r][ch ^ (r & 7)];
+            if (row >= row0 && row < rows_total)
+                *reinterpret_cast<uint4*>(co.out[mem] + (size_t)row * pitch + colbase + 16 * ch) = o;
         }
-        cp_async_wait<0>();
-    } else {
-        for (int row = rbeg; row < rend; ++row) {
-            const uint32_t* srow = base + (size_t)row * W;
-            uint32_t o[2] = {0, 0};
-#pragma unroll
-            for (int e = 0; e < 16; ++e) {
-                const int s = src[e];
-                if (s >= 0) o[e >> 3] |= ((__ldg(srow + (s >> 5)) >> (31 - (s & 31))) & 1u) << (4 * (e & 7) + 1);
-            }
-            if (kk0 < region) *reinterpret_cast<uint2*>(out + (size_t)row * pitch + colbase) = make_uint2(o[0], o[1]);
-        }
+        __syncwarp();
     }
 }
 
@@ -594,10 +618,10 @@ __device__ __forceinline__ void record_error(int* err, int code) { atomicCAS(err
 // each CTA holds the accumulators of its 128 A rows and scores them; triplets,
 // or pairs with TWO.  Without PAIR: the kind::i8 single-CTA kernel (pair
 // table).  STAGE: count segment 0 is copied out of TMEM early (triplets).
-// The pair kernel is held to 144 registers a thread: its ten warps then leave
-// room on every SM sub-partition for a warp of the regrouping kernels, which
-// run beside it on the auxiliary stream (at 168 registers they could not, and
-// the regrouping of the next group only ran in the gaps between launches).
+// One CTA of ten warps per SM: up to 168 registers a thread (three warps on
+// some SM sub-partition).  The regrouping kernel does not share its SMs (its
+// shared memory does not fit beside a counting CTA), so nothing else needs
+// them; at 144 the filtered K2 instances spilled and ran 2.5 % slower.
 // SC: the score fixed at compile time (0 = K2, 1 = MI) or -1 (read at run time).
 // TWO: the pair kernel scoring pairs (two class segments, two accumulator sets)
 // instead of counting triplets.
@@ -606,7 +630,7 @@ __device__ __forceinline__ void record_error(int* err, int code) { atomicCAS(err
 // CTA's current k-th candidate are scored exactly (from the global table),
 // so the candidate lists are those of scoring every set.
 template <bool PAIR, bool STAGE, int SC = -1, bool TWO = false, int VAR = 0>
-__global__ void __launch_bounds__(kThreads, 1) __maxnreg__(PAIR ? 144 : 200)
+__global__ void __launch_bounds__(kThreads, 1)
     tc_kernel(const __grid_constant__ TmapPack tm, const __grid_constant__ TcParams P) {
     static_assert(PAIR || !STAGE, "staging is a pair-kernel mode");
     static_assert(!TWO || (PAIR && !STAGE), "the 2-way pair kernel is the plain pair instance");
@@ -1329,6 +1353,7 @@ episdet_status tensor_pair_totals(Workspace* w, const uint32_t* d_planes, int M,
 }
 
 episdet_status tensor_init_attributes() {
+    CUDA_TRY(cudaFuncSetAttribute(regroup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kRgSmem));
     CUDA_TRY(cudaFuncSetAttribute(tc_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)KCfg<false, false>::kSmemTotal));
     CUDA_TRY(cudaFuncSetAttribute(tc_kernel<true, false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1482,27 +1507,30 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     {
         const size_t row_bytes = 2 * sizeof(uint4) * (size_t)M;  // one table row, both classes
         const size_t xrows_bytes = row_bytes * 2 * kTileSnps;
-        size_t other = (size_t)rows * pitch2 + (size_t)kXSets * kMaxGroup * rows * pitchx +
-                       (size_t)kXSets * kMaxGroup * (info_bytes + idx_bytes) + sizeof(Cand) * (size_t)kCapG * grid;
-        // Buffers this workspace already holds are reused (or replaced) below.
-        size_t held = w->pair4[0].cap + w->pair4[1].cap + w->pairx[0].cap + w->pairx[1].cap + w->planes8.cap +
-                      w->xinfo.cap + w->cbuf.cap;
-        for (const DevBuf& b : w->xsub) held += b.cap;
+        // The other buffers of the search first (their later ensure calls
+        // find them in place); the pair table gets what is left.
+        for (DevBuf& d : w->xsub) CUDA_TRY(d.ensure((size_t)rows * pitchx));
+        for (int c = 0; c < 2; ++c)
+            CUDA_TRY(w->planes_t[c].ensure(sizeof(uint32_t) * (size_t)D.W[c] * 32 * tt_row_words(rows)));
+        CUDA_TRY(w->xinfo.ensure((size_t)kXSets * kMaxGroup * (info_bytes + idx_bytes)));
+        CUDA_TRY(w->cbuf.ensure(sizeof(Cand) * (size_t)kCapG * grid));
         size_t fr = 0, tot = 0;
         CUDA_TRY(cudaMemGetInfo(&fr, &tot));
         // Left for the tile lists, slots, merge buffers and the driver.
         const size_t reserve = std::max<size_t>(tot / 32, (size_t)1 << 30);
+        // The pair-table buffers are replaced when they grow, so their memory counts as free.
+        const size_t held = w->pair4[0].cap + w->pair4[1].cap + w->pairx[0].cap + w->pairx[1].cap;
         const size_t avail = fr + held > reserve ? fr + held - reserve : 0;
         if (o.pair_block_snps > 0) {
             blk_tiles = std::min(blk_tiles, (o.pair_block_snps + 2 * kTileSnps - 1) / (2 * kTileSnps));
-        } else if (row_bytes * (size_t)M + other > avail) {
-            const size_t left = avail > other + xrows_bytes ? avail - other - xrows_bytes : 0;
+        } else if (row_bytes * (size_t)M > avail) {
+            const size_t left = avail > xrows_bytes ? avail - xrows_bytes : 0;
             blk_tiles = (int)std::min<size_t>((size_t)blk_tiles, left / (row_bytes * 2 * kTileSnps));
             if (blk_tiles < 1)
                 return set_error(EPISDET_ERR_OUT_OF_MEMORY,
-                                 "3-way search of %d SNPs: no 128-row block of the pair table fits beside the "
-                                 "%.1f GB of operand buffers",
-                                 M, (double)other / 1e9);
+                                 "3-way search of %d SNPs: no 128-row block of the pair table fits in the %.1f GB "
+                                 "left beside the operand buffers",
+                                 M, (double)avail / 1e9);
         }
     }
     const bool blocked = blk_tiles < nt2 - a_first;
@@ -1656,11 +1684,25 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
         pairs = std::min(pairs, grid / 2);
         if (pairs < 1) return set_error(EPISDET_ERR_UNSUPPORTED, "no CTA pair of the counting kernel fits on the device");
     }
-    // The regrouping reads the planes and marginals staged on st.
+    // Sample-major planes for the regrouping.
+    const int rwp = tt_row_words(rows);
+    for (int c = 0; c < 2; ++c) {
+        CUDA_TRY(w->planes_t[c].ensure(sizeof(uint32_t) * (size_t)D.W[c] * 32 * rwp));
+        const int warps = (rwp / 8) * (D.W[c] / 8);
+        transpose_planes_kernel<<<(warps + kTtThreads / 32 - 1) / (kTtThreads / 32), kTtThreads, 0, w->st>>>(
+            D, c, (uint32_t*)w->planes_t[c].p, rows, rwp);
+        CHECK_LAUNCH();
+        ++*launches;
+    }
+    // The regrouping reads the planes, their transposes and the marginals staged on st.
     CUDA_TRY(cudaEventRecord(w->ev_ready, w->st));
     CUDA_TRY(cudaStreamWaitEvent(w->aux_st, w->ev_ready, 0));
-    // Pair tiles each first SNP was counted against (for the MAC count).
-    std::vector<double> x_tiles(w->timing ? (size_t)M : 0, 0.0);
+    // Pair tiles each first SNP was counted against, per launch (for the MAC count).
+    struct LaunchTiles {
+        int x0, gn;
+        int len[kMaxGroup];
+    };
+    std::vector<LaunchTiles> launch_tiles;
     int gi = 0;
     int xt0 = -1;  // first row held in pairx (Y-blocked)
     for (int blk = 0; blk < nblk; ++blk) {
@@ -1679,6 +1721,7 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
             const int b = gi % kXSets;
             // (Kept aside until the launch: store_pairs below rewrites p.grp.)
             GroupDesc gdesc[kMaxGroup];
+            LaunchTiles lt{x0, gn, {0, 0, 0, 0}};
             int cum = 0;
             for (int g = 0; g < gn; ++g) {
                 const int x = x0 + g;
@@ -1686,9 +1729,10 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
                 const size_t li = (size_t)blk * (nt2 + 1) + (x + 1) / (2 * kTileSnps);
                 gdesc[g] = GroupDesc{d_lists + list_off[li], cum, x, d_info[b][g]};
                 cum += list_len[li];
-                if (w->timing) x_tiles[x] += list_len[li];
+                lt.len[g] = list_len[li];
             }
             if (cum == 0) continue;
+            if (w->timing) launch_tiles.push_back(lt);
             ++gi;
             if (blocked && (xt0 < 0 || x0 < xt0 || x0 + gn > xt0 + 2 * kTileSnps)) {
                 // X-Y and X-Z rows of this group's first SNPs (and the next ones').
@@ -1706,9 +1750,10 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
             CHECK_LAUNCH();
             for (int g = 0; g < gn; ++g)
                 co[b].row0[g] = kNPair * bfirst(std::max((x0 + g + 1) / (2 * kTileSnps), ya0));
-            const int max_rows = rows - co[b].row0[0];  // the first member needs the most rows
-            const dim3 cgrid(cmp_chunks(D.W[0]) + cmp_chunks(D.W[1]), (max_rows + kCmpRows - 1) / kCmpRows, gn);
-            compact_kernel<<<cgrid, kCmpThreads, 0, w->aux_st>>>(D, xw[b], co[b], rows, pitchx);
+            const dim3 rgrid((D.W[0] * 32 + kClassPad) / kF4PerKB + (D.W[1] * 32 + kClassPad) / kF4PerKB,
+                             (rows + kRgRows - 1) / kRgRows, gn);
+            regroup_kernel<<<rgrid, kRgThreads, kRgSmem, w->aux_st>>>(D, xw[b], co[b], (const uint32_t*)w->planes_t[0].p,
+                                                                (const uint32_t*)w->planes_t[1].p, rwp, rows, pitchx);
             CHECK_LAUNCH();
             CUDA_TRY(cudaEventRecord(w->ev_cmp[b], w->aux_st));
             CUDA_TRY(cudaStreamWaitEvent(w->st, w->ev_cmp[b], 0));
@@ -1752,8 +1797,7 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
         }
         CUDA_TRY(cudaStreamSynchronize(w->st));
         w->d2h += (int64_t)(2 * sizeof(int) * 3 * M);
-        double macs = 0.0;
-        for (int x = fb; x < xend; ++x) {
+        auto kext_of = [&](int x) {
             int tot[3];
             for (int g = 0; g < 3; ++g) tot[g] = mg[0][(size_t)g * M + x] + mg[1][(size_t)g * M + x];
             int gd = 0;
@@ -1763,7 +1807,14 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
             for (int c = 0; c < 2; ++c)
                 for (int g = 0; g < 3; ++g)
                     if (g != gd) kext += ((mg[c][(size_t)g * M + x] + kF4PerKB - 1) / kF4PerKB) * (long)kF4PerKB;
-            macs += x_tiles[x] * 2 * kTileRows * kNPair * (double)kext;
+            return kext;
+        };
+        double macs = 0.0;
+        for (const LaunchTiles& lt : launch_tiles) {
+            double m = 0.0;
+            for (int g = 0; g < lt.gn; ++g) m += (double)lt.len[g] * 2 * kTileRows * kNPair * (double)kext_of(lt.x0 + g);
+            w->launch_macs.push_back(m);
+            macs += m;
         }
         w->executed_macs = macs;
     }

@@ -48,7 +48,7 @@ EXPORTED = [
     "episdet_generate", "episdet_generate_cohort", "episdet_generate_labels", "episdet_n_choose_k",
     "episdet_status_string", "episdet_last_error", "episdet_abi_version", "episdet_release_workspace",
     "episdet_search_pairs_noalloc", "episdet_binarize", "episdet_perm_pvalues", "episdet_search_resumable",
-    "episdet_tuned_stage", "episdet_test_fail_allocation",
+    "episdet_tuned_stage", "episdet_test_fail_allocation", "episdet_last_launch_profile",
 ]
 
 
@@ -147,6 +147,8 @@ def lib() -> ctypes.CDLL:
     L.episdet_abi_version.restype = ctypes.c_int32
     L.episdet_release_workspace.argtypes = [ctypes.c_int32]
     L.episdet_release_workspace.restype = ctypes.c_int
+    L.episdet_last_launch_profile.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64]
+    L.episdet_last_launch_profile.restype = ctypes.c_int64
     L.episdet_test_fail_allocation.argtypes = [ctypes.c_int32]
     L.episdet_test_fail_allocation.restype = None
     L.episdet_search_pairs_noalloc.argtypes = [P(Dataset), P(Options), P(Result)]
@@ -374,6 +376,17 @@ def search_resumable(cases, controls, num_cases: int, num_controls: int, checkpo
 
 def release_workspace(device: int = 0) -> None:
     _check(lib().episdet_release_workspace(device))
+
+
+def last_launch_profile(device: int = 0):
+    """Per counting launch of the last search with FLAG_TIMING on `device`:
+    (device ms, tensor MACs issued), two float64 arrays in launch order."""
+    n = int(lib().episdet_last_launch_profile(device, None, None, 0))
+    ms = np.zeros(n, dtype=np.float64)
+    macs = np.zeros(n, dtype=np.float64)
+    if n:
+        lib().episdet_last_launch_profile(device, ms.ctypes.data, macs.ctypes.data, n)
+    return ms, macs
 
 
 def test_fail_allocation(after: int) -> None:
