@@ -535,17 +535,26 @@ constexpr int kRgRows = 1024;
 constexpr int kRgWords = kRgRows / 32;  // row words per position
 constexpr int kRgOutBytes = (kRgThreads / 32) * 32 * 8 * 16;
 constexpr int kRgTBytes = kRgThreads * (kRgWords + 1) * 4;
-constexpr int kRgSmem = kRgOutBytes + kRgTBytes + 256 * 4;
+constexpr int kRgSmem = kRgOutBytes + kRgTBytes;
+
+// e2m1 nibbles of 8 positions (bit e of b = position e): 1.0 = 2 in nibble e,
+// the even position in the low nibble of each byte.  Bit e moves to bit
+// 4 e + 1 by three shift-and-mask spreading steps.
+__device__ __forceinline__ uint32_t e2m1_nibbles8(uint32_t b) {
+    uint32_t v = (b | (b << 12)) & 0x000F000Fu;
+    v = (v | (v << 6)) & 0x03030303u;
+    v = (v | (v << 3)) & 0x11111111u;
+    return v << 1;
+}
 __global__ void __launch_bounds__(kRgThreads, 2)
     regroup_kernel(DevData D, XWork xw, CmpOut co, const uint32_t* __restrict__ tt0, const uint32_t* __restrict__ tt1,
                    int rwp, int rows_total, int pitch) {
     // Dynamic shared memory (kRgSmem bytes): per warp 32 rows x 8 chunks of 16
     // bytes (chunk j of row r at slot j ^ (r & 7)); [position][row word],
-    // padded against bank conflicts; the nibble table.
+    // padded against bank conflicts.
     extern __shared__ __align__(16) uint8_t rg_smem[];
     uint4(*s_out)[32][8] = reinterpret_cast<uint4(*)[32][8]>(rg_smem);
     uint32_t(*s_t)[kRgWords + 1] = reinterpret_cast<uint32_t(*)[kRgWords + 1]>(rg_smem + kRgOutBytes);
-    uint32_t* s_lut = reinterpret_cast<uint32_t*>(rg_smem + kRgOutBytes + kRgTBytes);
     const int mem = (int)blockIdx.z;
     const int rt = (int)blockIdx.y;
     const int row0 = co.row0[mem];
@@ -558,14 +567,6 @@ __global__ void __launch_bounds__(kRgThreads, 2)
     const int pa = ((la + kF4PerKB - 1) / kF4PerKB) * kF4PerKB, pb = ((lb + kF4PerKB - 1) / kF4PerKB) * kF4PerKB;
     if (k0 >= pa + pb) return;  // uniform over the CTA
     const int t = threadIdx.x;
-    // e2m1 nibbles of 8 positions (bit e of the index = position e): 1.0 = 2,
-    // the even position in the low nibble of each byte.
-    {
-        uint32_t v = 0;
-#pragma unroll
-        for (int e = 0; e < 8; ++e) v |= ((t >> e) & 1u) << (4 * e + 1);
-        s_lut[t] = v;
-    }
     const int k = k0 + t;
     const int* __restrict__ idx = xw.idx(mem) + (size_t)c * 2 * xw.max_n;
     int src = -1;
@@ -593,8 +594,8 @@ __global__ void __launch_bounds__(kRgThreads, 2)
             // Lane l: row word q at position 32 j + l; after the transpose,
             // lane k holds row 32 q + k with position 32 j + l at bit 31 - l.
             const uint32_t x = __brev(warp_transpose32(s_t[32 * j + lane][q], lane));
-            so[lane][j ^ (lane & 7)] =
-                make_uint4(s_lut[x & 255u], s_lut[(x >> 8) & 255u], s_lut[(x >> 16) & 255u], s_lut[x >> 24]);
+            so[lane][j ^ (lane & 7)] = make_uint4(e2m1_nibbles8(x & 255u), e2m1_nibbles8((x >> 8) & 255u),
+                                                  e2m1_nibbles8((x >> 16) & 255u), e2m1_nibbles8(x >> 24));
         }
         __syncwarp();
         // Store i: rows 4 i .. 4 i + 3 of the 32, eight lanes (16 bytes each) per row.
