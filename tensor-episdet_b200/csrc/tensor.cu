@@ -546,68 +546,116 @@ __device__ __forceinline__ uint32_t e2m1_nibbles8(uint32_t b) {
     v = (v | (v << 3)) & 0x11111111u;
     return v << 1;
 }
+// Persistent: a CTA claims work items (member, class K block, row tile) from
+// a launch-wide counter (*ctr, zero at launch), skipping those past a
+// member's region or below its first row, and loads the next item's source
+// samples into registers while it turns the current one into rows.  Claiming
+// (rather than a fixed share per CTA) balances the items over CTAs that start
+// late: the launch begins on the SMs the previous counting launch frees.
 __global__ void __launch_bounds__(kRgThreads, 2)
     regroup_kernel(DevData D, XWork xw, CmpOut co, const uint32_t* __restrict__ tt0, const uint32_t* __restrict__ tt1,
-                   int rwp, int rows_total, int pitch) {
+                   int rwp, int rows_total, int pitch, int nmem, int* __restrict__ ctr) {
     // Dynamic shared memory (kRgSmem bytes): per warp 32 rows x 8 chunks of 16
     // bytes (chunk j of row r at slot j ^ (r & 7)); [position][row word],
     // padded against bank conflicts.
     extern __shared__ __align__(16) uint8_t rg_smem[];
     uint4(*s_out)[32][8] = reinterpret_cast<uint4(*)[32][8]>(rg_smem);
     uint32_t(*s_t)[kRgWords + 1] = reinterpret_cast<uint32_t(*)[kRgWords + 1]>(rg_smem + kRgOutBytes);
-    const int mem = (int)blockIdx.z;
-    const int rt = (int)blockIdx.y;
-    const int row0 = co.row0[mem];
-    if ((rt + 1) * kRgRows <= row0 || rt * kRgRows >= rows_total) return;  // uniform over the CTA
-    const XInfo* __restrict__ info = xw.info(mem);
-    const int T0 = (D.W[0] * 32 + kClassPad) / kF4PerKB;
-    const int c = (int)blockIdx.x < T0 ? 0 : 1;
-    const int k0 = ((int)blockIdx.x - (c ? T0 : 0)) * kF4PerKB;
-    const int la = info->len[c][0], lb = info->len[c][1];
-    const int pa = ((la + kF4PerKB - 1) / kF4PerKB) * kF4PerKB, pb = ((lb + kF4PerKB - 1) / kF4PerKB) * kF4PerKB;
-    if (k0 >= pa + pb) return;  // uniform over the CTA
-    const int t = threadIdx.x;
-    const int k = k0 + t;
-    const int* __restrict__ idx = xw.idx(mem) + (size_t)c * 2 * xw.max_n;
-    int src = -1;
-    if (k < pa) {
-        if (k < la) src = __ldg(idx + k);
-    } else if (k - pa < lb) {
-        src = __ldg(idx + xw.max_n + (k - pa));
-    }
-    // Row words past the padded row count (the last tile) read as zero.
-    const int nw = min(kRgWords, rwp - rt * kRgWords);
-    const uint4* p = reinterpret_cast<const uint4*>((c ? tt1 : tt0) + (size_t)max(src, 0) * rwp + rt * kRgWords);
-#pragma unroll
-    for (int e = 0; e < kRgWords / 4; ++e) {
-        const uint4 v = (src >= 0 && 4 * e < nw) ? __ldg(p + e) : make_uint4(0, 0, 0, 0);
-        s_t[t][4 * e] = v.x, s_t[t][4 * e + 1] = v.y, s_t[t][4 * e + 2] = v.z, s_t[t][4 * e + 3] = v.w;
+    __shared__ int s_len[kMaxGroup][2][2];  // [member][class][segment]: samples
+    __shared__ int s_claim;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    if (t < 4 * nmem) {
+        const int m = t >> 2, c = (t >> 1) & 1, sg = t & 1;
+        s_len[m][c][sg] = xw.info(m)->len[c][sg];
     }
     __syncthreads();
-    const int lane = t & 31, w = t >> 5;
-    const int colbase = ((c ? D.W[0] * 32 + kClassPad : 0) + k0) / 2;
+    const int T0 = (D.W[0] * 32 + kClassPad) / kF4PerKB;
+    const int KT = T0 + (D.W[1] * 32 + kClassPad) / kF4PerKB;
+    const int RT = (rows_total + kRgRows - 1) / kRgRows;
+    const int nitems = nmem * KT * RT;
+    // Item i: row tile i % RT, K block (i / RT) % KT of the two class regions,
+    // member i / (RT * KT).  Invalid items are skipped (uniformly).
+    auto decode = [&](int i, int& m, int& c, int& k0, int& rt) -> bool {
+        rt = i % RT;
+        const int kt = (i / RT) % KT;
+        m = i / (RT * KT);
+        c = kt < T0 ? 0 : 1;
+        k0 = (kt - (c ? T0 : 0)) * kF4PerKB;
+        const int pa = (s_len[m][c][0] + kF4PerKB - 1) / kF4PerKB * kF4PerKB;
+        const int pb = (s_len[m][c][1] + kF4PerKB - 1) / kF4PerKB * kF4PerKB;
+        return k0 < pa + pb && (rt + 1) * kRgRows > co.row0[m];
+    };
+    // The next claimed item that is valid (nitems when none is left); called
+    // by every thread, between barriers on s_claim.
+    auto next_valid = [&](int& m, int& c, int& k0, int& rt) {
+        for (;;) {
+            if (t == 0) s_claim = atomicAdd(ctr, 1);
+            __syncthreads();
+            const int i = s_claim;
+            __syncthreads();
+            if (i >= nitems) return nitems;
+            if (decode(i, m, c, k0, rt)) return i;
+        }
+    };
+    // This thread's position of an item: its source sample's 128 bytes of the row tile.
+    auto load = [&](int m, int c, int k0, int rt, uint4 (&v)[kRgWords / 4]) {
+        const int la = s_len[m][c][0], pa = (la + kF4PerKB - 1) / kF4PerKB * kF4PerKB, lb = s_len[m][c][1];
+        const int k = k0 + t;
+        const int* __restrict__ idx = xw.idx(m) + (size_t)c * 2 * xw.max_n;
+        int src = -1;
+        if (k < pa) {
+            if (k < la) src = __ldg(idx + k);
+        } else if (k - pa < lb) {
+            src = __ldg(idx + xw.max_n + (k - pa));
+        }
+        // Row words past the padded row count (the last tile) read as zero.
+        const int nw = min(kRgWords, rwp - rt * kRgWords);
+        const uint4* p =
+            reinterpret_cast<const uint4*>((c ? tt1 : tt0) + (size_t)max(src, 0) * rwp + rt * kRgWords);
+#pragma unroll
+        for (int e = 0; e < kRgWords / 4; ++e)
+            v[e] = (src >= 0 && 4 * e < nw) ? __ldg(p + e) : make_uint4(0, 0, 0, 0);
+    };
+    int m, c, k0, rt;
+    int i = next_valid(m, c, k0, rt);
+    uint4 v[kRgWords / 4];
+    if (i < nitems) load(m, c, k0, rt, v);
     uint4(*so)[8] = s_out[w];
+    while (i < nitems) {
+#pragma unroll
+        for (int e = 0; e < kRgWords / 4; ++e) {
+            s_t[t][4 * e] = v[e].x, s_t[t][4 * e + 1] = v[e].y;
+            s_t[t][4 * e + 2] = v[e].z, s_t[t][4 * e + 3] = v[e].w;
+        }
+        __syncthreads();
+        const int cm = m, cc = c, ck0 = k0, crt = rt;
+        i = next_valid(m, c, k0, rt);
+        if (i < nitems) load(m, c, k0, rt, v);  // lands while this item is turned into rows
+        const int row0 = co.row0[cm];
+        uint8_t* __restrict__ out = co.out[cm] + ((cc ? D.W[0] * 32 + kClassPad : 0) + ck0) / 2;
 #pragma unroll 1
-    for (int q = w * (kRgWords / 8); q < (w + 1) * (kRgWords / 8); ++q) {
+        for (int q = w * (kRgWords / 8); q < (w + 1) * (kRgWords / 8); ++q) {
 #pragma unroll
-        for (int j = 0; j < kRgThreads / 32; ++j) {
-            // Lane l: row word q at position 32 j + l; after the transpose,
-            // lane k holds row 32 q + k with position 32 j + l at bit 31 - l.
-            const uint32_t x = __brev(warp_transpose32(s_t[32 * j + lane][q], lane));
-            so[lane][j ^ (lane & 7)] = make_uint4(e2m1_nibbles8(x & 255u), e2m1_nibbles8((x >> 8) & 255u),
-                                                  e2m1_nibbles8((x >> 16) & 255u), e2m1_nibbles8(x >> 24));
-        }
-        __syncwarp();
-        // Store i: rows 4 i .. 4 i + 3 of the 32, eight lanes (16 bytes each) per row.
+            for (int j = 0; j < kRgThreads / 32; ++j) {
+                // Lane l: row word q at position 32 j + l; after the transpose,
+                // lane k holds row 32 q + k with position 32 j + l at bit 31 - l.
+                const uint32_t x = __brev(warp_transpose32(s_t[32 * j + lane][q], lane));
+                so[lane][j ^ (lane & 7)] = make_uint4(e2m1_nibbles8(x & 255u), e2m1_nibbles8((x >> 8) & 255u),
+                                                      e2m1_nibbles8((x >> 16) & 255u), e2m1_nibbles8(x >> 24));
+            }
+            __syncwarp();
+            // Store i: rows 4 i .. 4 i + 3 of the 32, eight lanes (16 bytes each) per row.
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const int r = 4 * i + (lane >> 3), ch = lane & 7;
-            const int row = rt * kRgRows + q * 32 + r;
-            const uint4 o = so[r][ch ^ (r & 7)];
-            if (row >= row0 && row < rows_total)
-                *reinterpret_cast<uint4*>(co.out[mem] + (size_t)row * pitch + colbase + 16 * ch) = o;
+            for (int s4 = 0; s4 < 8; ++s4) {
+                const int r = 4 * s4 + (lane >> 3), ch = lane & 7;
+                const int row = crt * kRgRows + q * 32 + r;
+                const uint4 o = so[r][ch ^ (r & 7)];
+                if (row >= row0 && row < rows_total)
+                    *reinterpret_cast<uint4*>(out + (size_t)row * pitch + 16 * ch) = o;
+            }
+            __syncwarp();
         }
-        __syncwarp();
+        __syncthreads();  // s_t is refilled next
     }
 }
 
@@ -1685,8 +1733,13 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
         pairs = std::min(pairs, grid / 2);
         if (pairs < 1) return set_error(EPISDET_ERR_UNSUPPORTED, "no CTA pair of the counting kernel fits on the device");
     }
-    // Sample-major planes for the regrouping.
+    // Sample-major planes for the regrouping, and its persistent grid (as many
+    // CTAs as fit on the device at once).
     const int rwp = tt_row_words(rows);
+    int rg_per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rg_per_sm, regroup_kernel, kRgThreads, kRgSmem));
+    const int rg_ctas = std::max(1, rg_per_sm) * grid;
+    int* const rg_ctr = d_err + 2;  // the regrouping's item counter (reset before each launch)
     for (int c = 0; c < 2; ++c) {
         CUDA_TRY(w->planes_t[c].ensure(sizeof(uint32_t) * (size_t)D.W[c] * 32 * rwp));
         const int warps = (rwp / 8) * (D.W[c] / 8);
@@ -1751,10 +1804,10 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
             CHECK_LAUNCH();
             for (int g = 0; g < gn; ++g)
                 co[b].row0[g] = kNPair * bfirst(std::max((x0 + g + 1) / (2 * kTileSnps), ya0));
-            const dim3 rgrid((D.W[0] * 32 + kClassPad) / kF4PerKB + (D.W[1] * 32 + kClassPad) / kF4PerKB,
-                             (rows + kRgRows - 1) / kRgRows, gn);
-            regroup_kernel<<<rgrid, kRgThreads, kRgSmem, w->aux_st>>>(D, xw[b], co[b], (const uint32_t*)w->planes_t[0].p,
-                                                                (const uint32_t*)w->planes_t[1].p, rwp, rows, pitchx);
+            CUDA_TRY(cudaMemsetAsync(rg_ctr, 0, sizeof(int), w->aux_st));
+            regroup_kernel<<<rg_ctas, kRgThreads, kRgSmem, w->aux_st>>>(
+                D, xw[b], co[b], (const uint32_t*)w->planes_t[0].p, (const uint32_t*)w->planes_t[1].p, rwp, rows,
+                pitchx, gn, rg_ctr);
             CHECK_LAUNCH();
             CUDA_TRY(cudaEventRecord(w->ev_cmp[b], w->aux_st));
             CUDA_TRY(cudaStreamWaitEvent(w->st, w->ev_cmp[b], 0));
