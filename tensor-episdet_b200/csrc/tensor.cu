@@ -194,9 +194,10 @@ __device__ __forceinline__ bool drain_wait(uint64_t* bar, uint32_t parity, volat
 // Features of a kernel instance (a bit mask):
 //   kFeatFilter       K2 scoring filter (k2_approx32); only a 32-entry table in
 //                     shared memory;
-//   kFeatBigStages    stages of two K blocks (one MMA commit per 8 MMAs: a
+//   kFeatBigStages    stages of four K blocks (one MMA commit per 16 MMAs: a
 //                     commit costs the tensor pipe about as much as four MMAs
-//                     of this shape, profiles/tcgen05_mma_peak.md), three of them;
+//                     of this shape, profiles/tcgen05_mma_peak.md), two of them
+//                     (2 x 94 KB; three stages of two K blocks ran 2 % slower);
 //   kFeatGlobalCands  candidate buffer in a global per-CTA region, its fill
 //                     checked once per tile;
 //   kFeatOpPrefetch   operand K blocks prefetched into L2 ahead of the stage loads;
@@ -213,8 +214,8 @@ template <bool PAIR, bool STAGE = false, int FEAT = 0>
 struct Cfg {
     static constexpr bool FILTER = (FEAT & kFeatFilter) != 0;
     static constexpr bool GCANDS = (FEAT & kFeatGlobalCands) != 0;
-    static constexpr int kKbPerStage = (FEAT & kFeatBigStages) ? 2 : 1;
-    static constexpr int kStages = (FEAT & kFeatBigStages) ? 3 : 4;
+    static constexpr int kKbPerStage = (FEAT & kFeatBigStages) ? 4 : 1;
+    static constexpr int kStages = (FEAT & kFeatBigStages) ? 2 : 4;
     static constexpr int kBRows = PAIR ? kZSnpsPair : 128;
     static constexpr int kNSeg = PAIR ? kNPair : 128;      // accumulator columns per count segment
     static constexpr int kZSnps = PAIR ? kZSnpsPair : kTileSnps;  // B SNPs per tile
