@@ -522,21 +522,25 @@ __global__ void __launch_bounds__(kTtThreads) transpose_planes_kernel(DevData D,
 }
 
 // Regrouped operand rows for the members of one launch (the layout above),
-// from tt: a CTA covers kRgRows rows x 256 packed sample
-// positions (one K block) of one class region of one member.  Each thread
-// copies the 128 bytes of its position's source sample (these rows: one
-// cache line), then each warp turns 32 rows x 32 positions at a time back into
-// rows as e2m1 nibbles, collects the 128 bytes of each of its 32 rows in
-// shared memory and writes them as whole lines, 4 rows per store (a store of
-// 16 bytes into each of 32 rows a pitch apart ran at a third of the rate).
-// With 67 KB of shared memory its CTAs do not fit beside a counting CTA, so
-// they run on the SMs the previous counting launch has left.
+// from tt: a work item is kRgRows rows x 256 packed sample positions (one K
+// block) of one class region of one member.  Each thread copies the 128 bytes
+// of its position's source sample (these rows: one cache line) into shared
+// memory; then each lane transposes one 32 rows x 32 positions block in its
+// own registers (no shuffles) and writes its 32 rows' 16 bytes, the eight
+// lanes of the same rows writing whole 128-byte lines.
 constexpr int kRgThreads = 256;
 constexpr int kRgRows = 1024;
 constexpr int kRgWords = kRgRows / 32;  // row words per position
-constexpr int kRgOutBytes = (kRgThreads / 32) * 32 * 8 * 16;
-constexpr int kRgTBytes = kRgThreads * (kRgWords + 1) * 4;
-constexpr int kRgSmem = kRgOutBytes + kRgTBytes;
+// [position][row word] with 33 words a position and 4 more each 32 positions,
+// so that both the per-position writes and the per-block column reads (lanes
+// of 4 row words x 8 position blocks) are free of bank conflicts.
+__host__ __device__ constexpr int rg_slot(int pos, int q) { return pos * (kRgWords + 1) + 4 * (pos >> 5) + q; }
+constexpr int kRgTBytes = 4 * (rg_slot(kRgThreads - 1, kRgWords - 1) + 1);
+// The allocation also keeps the kernel's CTAs off the SMs of a running
+// counting CTA (172 KB): the regrouping ran beside the counting kernel at the
+// cost of 15 % of the counting rate, more than it saved.
+constexpr int kRgSmem = 64 * 1024;
+static_assert(kRgTBytes <= kRgSmem, "regroup tile");
 
 // e2m1 nibbles of 8 positions (bit e of b = position e): 1.0 = 2 in nibble e,
 // the even position in the low nibble of each byte.  Bit e moves to bit
@@ -547,6 +551,23 @@ __device__ __forceinline__ uint32_t e2m1_nibbles8(uint32_t b) {
     v = (v | (v << 3)) & 0x11111111u;
     return v << 1;
 }
+
+// 32 x 32 bit transpose of a[0..31] in place: afterwards bit 31 - l of a[k]
+// is what bit 31 - k of a[l] was (the block-swap transpose of H. S. Warren,
+// Hacker's Delight, 2nd ed., section 7-3).
+__device__ __forceinline__ void transpose32(uint32_t (&a)[32]) {
+    uint32_t m = 0x0000FFFFu;
+#pragma unroll
+    for (int j = 16; j != 0; j >>= 1, m ^= m << j) {
+#pragma unroll
+        for (int k = 0; k < 32; k = (k + j + 1) & ~j) {
+            const uint32_t t = (a[k] ^ (a[k + j] >> j)) & m;
+            a[k] ^= t;
+            a[k + j] ^= t << j;
+        }
+    }
+}
+
 // Persistent: a CTA claims work items (member, class K block, row tile) from
 // a launch-wide counter (*ctr, zero at launch), skipping those past a
 // member's region or below its first row, and loads the next item's source
@@ -556,13 +577,8 @@ __device__ __forceinline__ uint32_t e2m1_nibbles8(uint32_t b) {
 __global__ void __launch_bounds__(kRgThreads, 2)
     regroup_kernel(DevData D, XWork xw, CmpOut co, const uint32_t* __restrict__ tt0, const uint32_t* __restrict__ tt1,
                    int rwp, int rows_total, int pitch, int nmem, int* __restrict__ ctr) {
-    // Dynamic shared memory (kRgSmem bytes): per warp 32 rows x 8 chunks of 16
-    // bytes (chunk j of row r at slot j ^ (r & 7)); [position][row word],
-    // padded against bank conflicts.
-    extern __shared__ __align__(16) uint8_t rg_smem[];
-    uint4(*s_out)[32][8] = reinterpret_cast<uint4(*)[32][8]>(rg_smem);
-    uint32_t(*s_t)[kRgWords + 1] = reinterpret_cast<uint32_t(*)[kRgWords + 1]>(rg_smem + kRgOutBytes);
-    __shared__ int s_len[kMaxGroup][2][2];  // [member][class][segment]: samples
+    extern __shared__ __align__(16) uint32_t s_t[];  // rg_slot(position, row word)
+    __shared__ int s_len[kMaxGroup][2][2];           // [member][class][segment]: samples
     __shared__ int s_claim;
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     if (t < 4 * nmem) {
@@ -617,44 +633,40 @@ __global__ void __launch_bounds__(kRgThreads, 2)
         for (int e = 0; e < kRgWords / 4; ++e)
             v[e] = (src >= 0 && 4 * e < nw) ? __ldg(p + e) : make_uint4(0, 0, 0, 0);
     };
+    // This lane's block: row word q (rows 32 q .. 32 q + 31 of the tile) and
+    // positions 32 j .. 32 j + 31.
+    const int q = 4 * w + (lane >> 3), j = lane & 7;
     int m, c, k0, rt;
     int i = next_valid(m, c, k0, rt);
     uint4 v[kRgWords / 4];
     if (i < nitems) load(m, c, k0, rt, v);
-    uint4(*so)[8] = s_out[w];
     while (i < nitems) {
 #pragma unroll
         for (int e = 0; e < kRgWords / 4; ++e) {
-            s_t[t][4 * e] = v[e].x, s_t[t][4 * e + 1] = v[e].y;
-            s_t[t][4 * e + 2] = v[e].z, s_t[t][4 * e + 3] = v[e].w;
+            s_t[rg_slot(t, 4 * e)] = v[e].x, s_t[rg_slot(t, 4 * e + 1)] = v[e].y;
+            s_t[rg_slot(t, 4 * e + 2)] = v[e].z, s_t[rg_slot(t, 4 * e + 3)] = v[e].w;
         }
         __syncthreads();
         const int cm = m, cc = c, ck0 = k0, crt = rt;
         i = next_valid(m, c, k0, rt);
         if (i < nitems) load(m, c, k0, rt, v);  // lands while this item is turned into rows
+        uint32_t a[32];
+        // a[p]: bit 31 - r is row 32 q + r at position 32 j + p.
+#pragma unroll
+        for (int p = 0; p < 32; ++p) a[p] = s_t[rg_slot(32 * j + p, q)];
+        transpose32(a);  // a[r]: bit 31 - p is row 32 q + r at position 32 j + p
         const int row0 = co.row0[cm];
-        uint8_t* __restrict__ out = co.out[cm] + ((cc ? D.W[0] * 32 + kClassPad : 0) + ck0) / 2;
-#pragma unroll 1
-        for (int q = w * (kRgWords / 8); q < (w + 1) * (kRgWords / 8); ++q) {
+        uint8_t* __restrict__ out =
+            co.out[cm] + ((cc ? D.W[0] * 32 + kClassPad : 0) + ck0) / 2 + 16 * j;
+        const int rbase = crt * kRgRows + 32 * q;
 #pragma unroll
-            for (int j = 0; j < kRgThreads / 32; ++j) {
-                // Lane l: row word q at position 32 j + l; after the transpose,
-                // lane k holds row 32 q + k with position 32 j + l at bit 31 - l.
-                const uint32_t x = __brev(warp_transpose32(s_t[32 * j + lane][q], lane));
-                so[lane][j ^ (lane & 7)] = make_uint4(e2m1_nibbles8(x & 255u), e2m1_nibbles8((x >> 8) & 255u),
-                                                      e2m1_nibbles8((x >> 16) & 255u), e2m1_nibbles8(x >> 24));
-            }
-            __syncwarp();
-            // Store i: rows 4 i .. 4 i + 3 of the 32, eight lanes (16 bytes each) per row.
-#pragma unroll
-            for (int s4 = 0; s4 < 8; ++s4) {
-                const int r = 4 * s4 + (lane >> 3), ch = lane & 7;
-                const int row = crt * kRgRows + q * 32 + r;
-                const uint4 o = so[r][ch ^ (r & 7)];
-                if (row >= row0 && row < rows_total)
-                    *reinterpret_cast<uint4*>(out + (size_t)row * pitch + 16 * ch) = o;
-            }
-            __syncwarp();
+        for (int r = 0; r < 32; ++r) {
+            const uint32_t x = __brev(a[r]);
+            const int row = rbase + r;
+            if (row >= row0 && row < rows_total)
+                *reinterpret_cast<uint4*>(out + (size_t)row * pitch) =
+                    make_uint4(e2m1_nibbles8(x & 255u), e2m1_nibbles8((x >> 8) & 255u),
+                               e2m1_nibbles8((x >> 16) & 255u), e2m1_nibbles8(x >> 24));
         }
         __syncthreads();  // s_t is refilled next
     }
