@@ -200,10 +200,21 @@ __device__ __forceinline__ bool drain_wait(uint64_t* bar, uint32_t parity, volat
 //                     (2 x 94 KB; three stages of two K blocks ran 2 % slower);
 //   kFeatGlobalCands  candidate buffer in a global per-CTA region, its fill
 //                     checked once per tile;
+//   kFeatMidStages    stages of two K blocks (one commit per 8 MMAs), three of
+//                     them: for the MI instance, whose exact scoring keeps a
+//                     32 KB table in shared memory (5 % faster than four
+//                     stages of one K block on the 8192 x 65536 MI workload);
 //   kFeatOpPrefetch   operand K blocks prefetched into L2 ahead of the stage loads;
 //   kFeatPairPrefetch the Y-Z and X-Z pair-table rows of a tile prefetched into
 //                     L2 while its MMAs run.
-enum : int { kFeatFilter = 1, kFeatBigStages = 2, kFeatGlobalCands = 4, kFeatOpPrefetch = 8, kFeatPairPrefetch = 16 };
+enum : int {
+    kFeatFilter = 1,
+    kFeatBigStages = 2,
+    kFeatGlobalCands = 4,
+    kFeatOpPrefetch = 8,
+    kFeatPairPrefetch = 16,
+    kFeatMidStages = 32
+};
 
 // Shared-memory layout of tc_kernel<PAIR, STAGE, FEAT>.  A K block holds
 // 128 bytes of this CTA's 128 A rows and of its B rows: all 128 for one CTA,
@@ -214,8 +225,8 @@ template <bool PAIR, bool STAGE = false, int FEAT = 0>
 struct Cfg {
     static constexpr bool FILTER = (FEAT & kFeatFilter) != 0;
     static constexpr bool GCANDS = (FEAT & kFeatGlobalCands) != 0;
-    static constexpr int kKbPerStage = (FEAT & kFeatBigStages) ? 4 : 1;
-    static constexpr int kStages = (FEAT & kFeatBigStages) ? 2 : 4;
+    static constexpr int kKbPerStage = (FEAT & kFeatBigStages) ? 4 : (FEAT & kFeatMidStages) ? 2 : 1;
+    static constexpr int kStages = (FEAT & kFeatBigStages) ? 2 : (FEAT & kFeatMidStages) ? 3 : 4;
     static constexpr int kBRows = PAIR ? kZSnpsPair : 128;
     static constexpr int kNSeg = PAIR ? kNPair : 128;      // accumulator columns per count segment
     static constexpr int kZSnps = PAIR ? kZSnpsPair : kTileSnps;  // B SNPs per tile
@@ -243,11 +254,12 @@ struct Cfg {
 
 // The configuration of one kernel instance, used by the kernel and by every
 // host-side launch and attribute, so the two can never disagree on the layout.
-// The K2 triplet instances (the headline search) filter, run stages of two K
-// blocks, keep their candidates in global memory and prefetch their pair-table
-// rows; operand prefetch (kFeatOpPrefetch) measured slower and is off.  The MI
-// triplet, 2-way and pair-table instances keep the plain layout (with MI's
-// exact scoring, larger stages cost the epilogue more L1 than they gained).
+// The K2 triplet instances of large searches (the headline search) filter,
+// run stages of four K blocks, keep their candidates in global memory and
+// prefetch their pair-table rows; operand prefetch (kFeatOpPrefetch) measured
+// slower and is off.  The MI triplet instances run stages of two K blocks with
+// their candidates in global memory; the 2-way and pair-table instances keep
+// the plain layout.
 // VAR = 1 selects these features for a K2 triplet instance; the host runs it
 // for searches large enough that each CTA scores far more sets than its
 // candidate list holds (kFilterMinSetsPerCta), and the plain K2 instance
@@ -257,7 +269,8 @@ struct Cfg {
 template <bool PAIR, bool TWO, int SC, int VAR>
 constexpr int kInstanceFeat = (PAIR && !TWO && SC == 0 && VAR == 1)
                                   ? (kFeatFilter | kFeatBigStages | kFeatGlobalCands | kFeatPairPrefetch)
-                                  : 0;
+                              : (PAIR && !TWO && SC == 1) ? (kFeatMidStages | kFeatGlobalCands)
+                                                          : 0;
 template <bool PAIR, bool STAGE, int SC = -1, bool TWO = false, int VAR = 0>
 using KCfg = Cfg<PAIR, STAGE, kInstanceFeat<PAIR, TWO, SC, VAR>>;
 constexpr double kFilterMinSetsPerCta = 1.0e7;
