@@ -201,9 +201,10 @@ __device__ __forceinline__ bool drain_wait(uint64_t* bar, uint32_t parity, volat
 //   kFeatGlobalCands  candidate buffer in a global per-CTA region, its fill
 //                     checked once per tile;
 //   kFeatMidStages    stages of two K blocks (one commit per 8 MMAs), three of
-//                     them: for the MI instance, whose exact scoring keeps a
-//                     32 KB table in shared memory (5 % faster than four
-//                     stages of one K block on the 8192 x 65536 MI workload);
+//                     them: for the MI triplet instance, whose exact scoring
+//                     keeps a 32 KB table in shared memory (5 % faster than
+//                     four stages of one K block on the 8192 x 65536 MI
+//                     workload), and the 2-way instances;
 //   kFeatOpPrefetch   operand K blocks prefetched into L2 ahead of the stage loads;
 //   kFeatPairPrefetch the Y-Z and X-Z pair-table rows of a tile prefetched into
 //                     L2 while its MMAs run.
@@ -258,8 +259,10 @@ struct Cfg {
 // run stages of four K blocks, keep their candidates in global memory and
 // prefetch their pair-table rows; operand prefetch (kFeatOpPrefetch) measured
 // slower and is off.  The MI triplet instances run stages of two K blocks with
-// their candidates in global memory; the 2-way and pair-table instances keep
-// the plain layout.
+// their candidates in global memory, the 2-way instances stages of two K
+// blocks (15 % faster on 16384 SNPs x 32768 samples); the exact K2 triplet and
+// pair-table instances keep the plain layout (stages of two K blocks were 3 %
+// slower for exact K2 triplets).
 // VAR = 1 selects these features for a K2 triplet instance; the host runs it
 // for searches large enough that each CTA scores far more sets than its
 // candidate list holds (kFilterMinSetsPerCta), and the plain K2 instance
@@ -270,6 +273,7 @@ template <bool PAIR, bool TWO, int SC, int VAR>
 constexpr int kInstanceFeat = (PAIR && !TWO && SC == 0 && VAR == 1)
                                   ? (kFeatFilter | kFeatBigStages | kFeatGlobalCands | kFeatPairPrefetch)
                               : (PAIR && !TWO && SC == 1) ? (kFeatMidStages | kFeatGlobalCands)
+                              : (PAIR && TWO)             ? kFeatMidStages
                                                           : 0;
 template <bool PAIR, bool STAGE, int SC = -1, bool TWO = false, int VAR = 0>
 using KCfg = Cfg<PAIR, STAGE, kInstanceFeat<PAIR, TWO, SC, VAR>>;
@@ -1697,7 +1701,9 @@ episdet_status run_tensor(Workspace* w, DevData& D, const ScoreTables& T, const 
     // Regrouped operands of the kMaxGroup X values of a launch, and their segment tables.
     for (int i = 0; i < kXSets * kMaxGroup; ++i) CUDA_TRY(w->xsub[i].ensure((size_t)rows * pitchx));
     // kXSets sets of regrouped operands and segment tables: the regrouping of
-    // the next groups (on aux_st) overlaps the counting launch of group g (on st).
+    // group g + 1 (on aux_st) is queued while the counting launch of group g
+    // (on st) runs and starts on the SMs that launch frees at its end, while
+    // its last tiles still read group g's set.
     CUDA_TRY(w->xinfo.ensure(kXSets * kMaxGroup * (info_bytes + idx_bytes)));
     TmapPack tmx[kXSets];
     XInfo* d_info[kXSets][kMaxGroup];
