@@ -192,3 +192,58 @@ def test_tables_equal_direct_counts_on_random_data(oracle):
         assert cs3.reshape(9, 3).sum(axis=1).tolist() == cs2.tolist()
         assert cn3.reshape(9, 3).sum(axis=1).tolist() == cn2.tolist()
         assert cs3.reshape(3, 9).sum(axis=1).tolist() == m_cases[:, x].tolist()
+
+
+def _round_f32(x):
+    """Exact rational x rounded to the nearest float32 (ties to even)."""
+    from fractions import Fraction
+
+    f = np.float32(float(x))
+    best = None
+    for c in (np.nextafter(f, np.float32(-np.inf)), f, np.nextafter(f, np.float32(np.inf))):
+        d = abs(Fraction(float(c)) - x)
+        key = (d, int(np.array([c], dtype=np.float32).view(np.uint32)[0]) & 1)
+        if best is None or key < best[0]:
+            best = (key, c)
+    return np.float32(best[1])
+
+
+def test_mi_fp32_score_follows_the_references_evaluation_order(oracle):
+    """The oracle's FP32 MI score is the reference's device arithmetic
+    (include/scoring.hpp:9-16, :18-51): per cell p = n * (1/N) in float and
+    fused multiply-adds into the two entropies, and H(Y) as the device
+    evaluates scoring.hpp:29-30 (float p, a double product rounded to float,
+    then a double multiply-add rounded to float).  Emulated here exactly with
+    rationals for the best pair of a dataset whose class sizes (2990, 4990)
+    round H(Y) differently from a double evaluation."""
+    from fractions import Fraction as F
+
+    nc, nn = 2990, 4990
+    N = nc + nn
+    inv = np.float32(1.0 / N)
+    t32 = lambda v: np.float32(0.0) if v == 0 else np.float32(math.log2(float(v) * float(inv)))
+    p1 = np.float32(np.float32(nc) * inv)
+    hy = np.float32(-(float(p1) * float(t32(nc))))
+    p2 = np.float32(np.float32(nn) * inv)
+    hy = np.float32(float(F(float(hy)) - F(float(p2)) * F(float(t32(nn)))))
+    hy_double = np.float32(-(nc / N * math.log2(nc / N)) - (nn / N * math.log2(nn / N)))
+    assert hy != hy_double  # the case discriminates between the two orders
+
+    cases, controls = oracle.generate(11, 40, nc, nn)
+    o = oracle.search(cases, controls, nc, nn, order=2, score="mi", top_k=4)
+    a, b = o["top"][0]
+    cs, cn = oracle.table2(cases, controls, nc, nn, a, b)
+
+    def fmaf(x, y, z):
+        return _round_f32(F(float(x)) * F(float(y)) + F(float(z)))
+
+    ha = np.float32(0.0)
+    hx = np.float32(0.0)
+    for s_, n_ in zip(cs.tolist(), cn.tolist()):
+        pc = np.float32(np.float32(s_) * inv)
+        ha = fmaf(-pc, t32(s_), ha)
+        pn = np.float32(np.float32(n_) * inv)
+        ha = fmaf(-pn, t32(n_), ha)
+        hx = fmaf(-np.float32(pc + pn), t32(s_ + n_), hx)
+    score = np.float32(np.float32(hx + hy) - ha)
+    assert np.array([score], dtype=np.float32).view(np.uint32)[0] == o["top_fp32"][:1].view(np.uint32)[0]
